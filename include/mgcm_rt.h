@@ -1,0 +1,181 @@
+/*
+ * mgcm_rt.h -- C ABI of the B200 column radiative transfer for the NASA Ames
+ * Legacy Mars GCM (v24).
+ *
+ * One batched call replaces the per-column radiation calls the reference
+ * makes inside the physics column loop of COMP3 (code/comp3.f:411-1044):
+ *
+ *   code/comp3.f:658    CALL OPTCV   (visible opacities; code/optcv.f90:1)
+ *   code/comp3.f:664    CUMTAUV store
+ *   code/comp3.f:672    CALL SFLUXV  (visible two-stream; code/sfluxv.f90:1,
+ *                                    code/gfluxv.f90:1, code/getdetau.f90:1,
+ *                                    code/dsolver.f90:1, code/dtridgl.f90:1)
+ *   code/comp3.f:677    SUNTOT divergences
+ *   code/comp3.f:724    CALL OPTCI   (IR opacities; code/optci.f90:1)
+ *   code/comp3.f:731    CALL SFLUXI  (IR two-stream; code/sfluxi.f90:1,
+ *                                    code/gfluxi.f90:1)
+ *   code/comp3.f:735    IRTOTAL divergences
+ *   code/comp3.f:698-747 surface / top-of-atmosphere diagnostics
+ *   code/comp3.f:765-771 QRAD heating rates (non-LTE factor included)
+ *
+ * Units are the reference's: pressures in mbar, temperatures in K, fluxes in
+ * W/m^2, QRAD in K/s of potential temperature (QRAD*OM is dT/dt).
+ *
+ * Layout: every per-column array has the column index slowest, so a Fortran
+ * host passes A(level, col) / A(level, band, col) / A(nw, ng, col) directly.
+ *   LEV  = 2L+3 (L_LEVELS)        level arrays     [ncol][LEV]
+ *   LEV1 = 2L+4 (L_LEVELS+1)      level+1 arrays   [ncol][LEV1]
+ *   band arrays                   [ncol][NB][LEV1] (NB = 7 visible, 5 IR)
+ *   NLAY = L+1 (L_NLAYRAD)        layer outputs    [ncol][NLAY]
+ *   DETAU, CUMTAUV                [ncol][17][7]    (Fortran A(nw,ng,col))
+ *
+ * Errors are negative return codes (never abort/exit; the reference STOPs,
+ * code/gfluxi.f90:215).  A handle is thread-safe: calls on one handle are
+ * serialised by an internal lock and run on the handle's own CUDA stream.
+ */
+#ifndef MGCM_RT_H
+#define MGCM_RT_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MGCM_RT_NSPECTV 7    /* L_NSPECTV, code/modules.f90:224 */
+#define MGCM_RT_NSPECTI 5    /* L_NSPECTI, code/modules.f90:223 */
+#define MGCM_RT_NGAUSS 17    /* L_NGAUSS,  code/modules.f90:225 */
+#define MGCM_RT_MAX_LAYERS 99 /* NLL <= NLP = 101, code/gfluxi.f90:193,215 */
+
+/* precision modes */
+#define MGCM_RT_FP64 0  /* plain FP64, operation order of the reference */
+#define MGCM_RT_MIXED 1 /* FP32 opacities/optics, FP64 solves and flux sums */
+
+/* status codes */
+#define MGCM_RT_OK 0
+#define MGCM_RT_EINVAL -1     /* null pointer, ncol < 0, bad config */
+#define MGCM_RT_ENONFINITE -2 /* NaN/Inf or non-positive pressure in an input */
+#define MGCM_RT_ETEMP -3      /* a temperature outside the Planck table [50,900) K */
+#define MGCM_RT_ELAYERS -4    /* L outside 1..MGCM_RT_MAX_LAYERS or above max_layers */
+#define MGCM_RT_ENOMEM -5     /* device memory or HBM budget exhausted */
+#define MGCM_RT_EIO -6        /* data file missing or malformed */
+#define MGCM_RT_ECUDA -7      /* CUDA runtime error */
+#define MGCM_RT_ETIMEOUT -8   /* wait() ran out of time */
+#define MGCM_RT_EBUSY -9      /* request queue full */
+#define MGCM_RT_ENOTFOUND -10 /* unknown or already collected ticket */
+
+typedef struct mgcm_rt_handle mgcm_rt_handle;
+
+typedef struct {
+    int max_layers;       /* largest L any batch will use (1..99) */
+    int precision;        /* MGCM_RT_FP64 or MGCM_RT_MIXED */
+    int device;           /* CUDA device ordinal */
+    int validate;         /* nonzero: check inputs (finite, T range) before each launch */
+    size_t hbm_budget;    /* device bytes for batch staging; 0 = 3/4 of free memory */
+} mgcm_rt_config;
+
+/* One batch of columns on one vertical grid. */
+typedef struct {
+    int ncol;             /* number of columns (>= 0) */
+    int nlayers;          /* L: GCM layers of this grid */
+    int device_ptrs;      /* nonzero: every array below is a device pointer */
+    double ptrop;         /* PTROP, mbar */
+    const double *sigma;  /* [LEV] SIGMA(K) of the grid (SIGMA(1)=SIGMA(2)=0) */
+    const double *sol;    /* [7] SOLARF/RSDIST, W/m^2 (code/comp3.f:300-304) */
+    const double *plev, *tlev, *pmid, *tmid, *qh2o;   /* [ncol][LEV]  (FILLPT, QH2O) */
+    const double *tauref, *qextrefdst;                 /* [ncol][LEV1] dust */
+    const double *qxvdst, *qsvdst, *gvdst;             /* [ncol][7][LEV1] */
+    const double *qxidst, *qsidst, *gidst;             /* [ncol][5][LEV1] */
+    const double *taurefcld, *qextrefcld;              /* [ncol][LEV1]; NULL = CLOUDON off */
+    const double *qxvcld, *qsvcld, *gvcld;             /* [ncol][7][LEV1] (with cloud) */
+    const double *qxicld, *qsicld, *gicld;             /* [ncol][5][LEV1] (with cloud) */
+    const double *acosz;  /* [ncol] cos(solar zenith); day when >= 1.0e-5 (REAL*4) */
+    const double *als;    /* [ncol] visible surface albedo */
+    const double *albi;   /* [ncol] IR surface albedo = 1 - emissivity */
+    const double *pcol;   /* [ncol] P(J,I) = surface pressure - PTROP, mbar */
+    double *detau;        /* [ncol][17][7] in/out: delta-Eddington surface tau; kept for night */
+    double *cumtauv;      /* [ncol][17][7] in/out: TAUCUMV(L_LEVELS); kept for night */
+} mgcm_rt_batch_in;
+
+typedef struct {
+    double *fmnetv, *fluxupv, *fluxdnv;  /* [ncol][NLAY] visible net/up/down midpoint fluxes */
+    double *fmneti, *fluxupi, *fluxdni;  /* [ncol][NLAY] IR */
+    double *suntot, *irtotal;            /* [ncol][NLAY] SUNTOT(2l+1), IRTOTAL(2l+1) */
+    double *qrad;                        /* [ncol][NLAY] QRAD(2l), K/s */
+    double *nfluxtopv, *nfluxtopi;       /* [ncol] */
+    double *diffvt;                      /* [ncol] diffuse visible down at the surface */
+    double *dnvflux, *dndiffv;           /* [ncol] DNVFLUX = FLUXDNV(NLAY), DNDIFFV = DIFFVT */
+    double *dnirflux, *fluxsurf;         /* [ncol] FLUXDNI(NLAY), (1-ALS)*FLUXDNV(NLAY) */
+} mgcm_rt_batch_out;
+
+/* Per-call statistics of the last completed run on a handle. */
+typedef struct {
+    double gpu_ms;          /* device time of the radiation kernels */
+    double total_ms;        /* host wall time of the call */
+    long long columns;      /* columns processed */
+    long long systems;      /* two-stream systems solved (after TLIMIT and night skips) */
+    int kernels;            /* kernels launched */
+    int status;             /* device status word (0 = clean) */
+} mgcm_rt_stats;
+
+/* Reads CO2H2O_{V,IR}_12_95_INTEL from data_dir (code/laginterp.f90:220-230),
+ * builds the k tables (code/setrad.f90, code/laginterp.f90), the Planck table
+ * (code/setspi.f90:245-259) and the band constants (code/setspv.f90), and
+ * uploads them.  Replaces RADSETUP (code/radsetup.f90:26-43).
+ * Returns NULL and sets *status on failure. */
+mgcm_rt_handle *mgcm_rt_create(const mgcm_rt_config *cfg, const char *data_dir, int *status);
+
+/* Synchronous batched radiation (the block code/comp3.f:637-771 for every
+ * column).  Host or device pointers per in->device_ptrs; outputs follow the
+ * same kind.  Night columns leave DETAU and CUMTAUV unchanged and report
+ * zero visible fluxes. */
+int mgcm_rt_run(mgcm_rt_handle *h, const mgcm_rt_batch_in *in, mgcm_rt_batch_out *out);
+
+/* Asynchronous form for device pointers: enqueue the batch on the handle's
+ * stream and return; mgcm_rt_sync() waits and returns the batch status.
+ * Lets a C/C++/Python host overlap its own work or capture a CUDA graph. */
+int mgcm_rt_enqueue(mgcm_rt_handle *h, const mgcm_rt_batch_in *in, mgcm_rt_batch_out *out);
+int mgcm_rt_sync(mgcm_rt_handle *h);
+
+/* Run the handle's work on a caller-owned cudaStream_t (NULL restores the
+ * handle's own stream). */
+int mgcm_rt_set_stream(mgcm_rt_handle *h, void *cuda_stream);
+
+/* Uneven batch: nbatch grids of different L and sizes in one persistent
+ * launch.  Every batch must use the same pointer kind. */
+int mgcm_rt_run_multi(mgcm_rt_handle *h, int nbatch, const mgcm_rt_batch_in *in,
+                      mgcm_rt_batch_out *out);
+
+/* Serving: queue a batch (pointers must stay valid until collected), get a
+ * ticket.  Requests are admitted against the HBM budget and run
+ * concurrently on the device as memory frees up. */
+int mgcm_rt_submit(mgcm_rt_handle *h, const mgcm_rt_batch_in *in, mgcm_rt_batch_out *out,
+                   long long *ticket);
+/* 1 = finished (result available), 0 = pending, < 0 = error for the ticket. */
+int mgcm_rt_poll(mgcm_rt_handle *h, long long ticket);
+/* Blocks until the ticket finishes or timeout_s passes (<0: no limit);
+ * returns the request's status and releases the ticket. */
+int mgcm_rt_wait(mgcm_rt_handle *h, long long ticket, double timeout_s);
+
+/* Partial radiation between full calls: DNVFLUX = DNDIFFV + direct beam from
+ * DETAU (code/dsolflux.f:28-45, code/comp3.f:320-351). */
+int mgcm_rt_dsolflux(mgcm_rt_handle *h, int ncol, int device_ptrs, const double *sol,
+                     const double *acosz, const double *detau, const double *dndiffv,
+                     double *dnvflux);
+
+int mgcm_rt_get_stats(mgcm_rt_handle *h, mgcm_rt_stats *st);
+
+/* Host copies of the set-up tables, laid out as the reference modules hold
+ * them: co2v (7,51,10,7,17) and co2i (7,51,10,5,17) Fortran order, planckir
+ * (5,8501), pfgasref (51).  Any pointer may be NULL.  No device needed. */
+int mgcm_rt_tables_host(const char *data_dir, double *co2v, double *co2i, double *planckir,
+                        double *pfgasref);
+
+void mgcm_rt_destroy(mgcm_rt_handle *h);
+const char *mgcm_rt_strerror(int status);
+const char *mgcm_rt_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MGCM_RT_H */

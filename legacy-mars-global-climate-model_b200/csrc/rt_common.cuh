@@ -1,0 +1,69 @@
+// Device-side definitions shared by the radiation kernels.
+#pragma once
+#include <cstdint>
+
+namespace mgcm {
+
+constexpr int D_NV = 7, D_NI = 5, D_NG = 17, D_NGK = 16, D_NT = 7, D_NP = 51, D_NH = 10;
+constexpr int D_NPLANCK = 8501;
+constexpr int D_MAXL = 99;
+constexpr int D_MAXNL = D_MAXL + 1;        // NLAYRAD
+constexpr int D_MAXLEV = 2 * D_MAXL + 3;   // L_LEVELS
+constexpr int NSYS_V = D_NV * D_NG;        // 119 visible systems per column
+constexpr int NSYS_I = D_NI * D_NG;        // 85 IR systems per column
+constexpr int NSYS = NSYS_V + NSYS_I;      // 204
+constexpr int NREFV_IDX = 5;               // L_NREFV = 6 (0.67 um band), 0-based
+
+// device status bits (OR-ed into the status word)
+constexpr uint32_t ST_PLANCK_RANGE = 1u;   // a Planck index left 1..8501 (clamped)
+constexpr uint32_t ST_NONFINITE = 2u;      // validation: NaN/Inf or p <= 0 in an input
+constexpr uint32_t ST_TEMP = 4u;           // validation: T outside [50,900)
+constexpr uint32_t ST_BADL = 8u;           // a segment with L outside 1..99
+
+// Constant tables (radcommon_h and friends).
+struct RtConst {
+    double tauray[D_NV];
+    double fzerov[D_NV];
+    double fzeroi[D_NI];
+    double gweight[D_NG];
+    double dwni[D_NI];
+    double pfgasref[D_NP];
+    double plimit[D_NP];     // bin search limits: log10(p) <= pfgasref[n] <=> p <= plimit[n]
+    double wrefh2o[D_NH];
+};
+
+// Pointers of one batch (one vertical grid) on the device.
+struct SegDev {
+    int ncol, L;
+    int col0;                 // first global column index of this segment (multi-grid)
+    double ptrop;
+    const double *sigma, *sol;
+    const double *plev, *tlev, *pmid, *tmid, *qh2o;
+    const double *tauref, *qextrefdst, *taurefcld, *qextrefcld;
+    const double *qxvdst, *qsvdst, *gvdst, *qxidst, *qsidst, *gidst;
+    const double *qxvcld, *qsvcld, *gvcld, *qxicld, *qsicld, *gicld;
+    const double *acosz, *als, *albi, *pcol;
+    double *detau, *cumtauv;
+    double *fmnetv, *fluxupv, *fluxdnv, *fmneti, *fluxupi, *fluxdni;
+    double *suntot, *irtotal, *qrad;
+    double *nfluxtopv, *nfluxtopi, *diffvt, *dnvflux, *dndiffv, *dnirflux, *fluxsurf;
+};
+
+constexpr int MAX_SEGS = 64;
+
+struct SegTable {
+    int nseg;
+    int total_cols;
+    SegDev seg[MAX_SEGS];
+};
+
+// Device-resident tables.
+struct TabDev {
+    const double *kv;        // [7][7][51][10][16] FP64, Gauss point fastest
+    const double *ki;        // [5][7][51][10][16]
+    const float *kvf;        // FP32 copies for the mixed path
+    const float *kif;
+    const double *planck;    // [8501][5]
+};
+
+}  // namespace mgcm

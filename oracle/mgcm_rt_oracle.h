@@ -1,0 +1,119 @@
+/*
+ * mgcm_rt_oracle.h -- CPU oracle for the column radiative transfer of the
+ * NASA Ames Legacy Mars GCM (v24).
+ *
+ * TEST INFRASTRUCTURE ONLY.  This is the checker the CUDA path is compared
+ * against; it is never linked into the product library.  Only tests/,
+ * __graft_entry__.smoke() and bench.py (its cpu_baseline leg and the
+ * reference arm) load it.
+ *
+ * It restates, line by line and in FP64, the reference Fortran of the hot
+ * path (code/tpindex.f90, optcv.f90, optci.f90, getdetau.f90, sfluxv.f90,
+ * gfluxv.f90, sfluxi.f90, gfluxi.f90, dsolver.f90, dtridgl.f90, dsolflux.f,
+ * the heating block of comp3.f:664-782) and its set-up (laginterp.f90,
+ * lagrange.f90, setspv.f90, setspi.f90, setrad.f90), with the number of GCM
+ * layers L a run-time value instead of the compile-time L_LAYERS.
+ *
+ * Array layout of a batch: the column index is slowest everywhere.
+ *   level arrays      [ncol][2L+3]         PLEV TLEV PMID TMID QH2O
+ *   level+1 arrays    [ncol][2L+4]         TAUREF QEXTREFDST TAUREFCLD QEXTREFCLD
+ *   band arrays       [ncol][NB][2L+4]     QXVDST ... (Fortran A(level,band))
+ *   layer outputs     [ncol][L+1]
+ *   DETAU / CUMTAUV   [ncol][17][7]        (Fortran A(nw,ng), nw fastest)
+ */
+#ifndef MGCM_RT_ORACLE_H
+#define MGCM_RT_ORACLE_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ORC_NSPECTV 7
+#define ORC_NSPECTI 5
+#define ORC_NGAUSS 17
+#define ORC_NTREF 7
+#define ORC_NPREF 11
+#define ORC_PINT 51
+#define ORC_REFH2O 10
+#define ORC_NPLANCK 8501
+#define ORC_MAXL 99
+
+typedef struct {
+    /* CO2V(nt,np,nh,nw,ng) in Fortran order: index nt + 7*(np + 51*(nh + 10*(nw + NB*ng))) */
+    double co2v[ORC_NTREF * ORC_PINT * ORC_REFH2O * ORC_NSPECTV * ORC_NGAUSS];
+    double co2i[ORC_NTREF * ORC_PINT * ORC_REFH2O * ORC_NSPECTI * ORC_NGAUSS];
+    double fzerov[ORC_NSPECTV];
+    double fzeroi[ORC_NSPECTI];
+    double pfgasref[ORC_PINT];
+    double tgasref[ORC_NTREF];
+    double pgasref[ORC_NPREF];
+    /* planckir(nw, it), it = 1..8501  ->  planckir[(it-1)*5 + nw-1] */
+    double planckir[ORC_NSPECTI * ORC_NPLANCK];
+    double wnov[ORC_NSPECTV], dwnv[ORC_NSPECTV], wavev[ORC_NSPECTV];
+    double solarf[ORC_NSPECTV], tauray[ORC_NSPECTV];
+    double wnoi[ORC_NSPECTI], dwni[ORC_NSPECTI], wavei[ORC_NSPECTI];
+    double qextv[ORC_NSPECTV], qscatv[ORC_NSPECTV], gv[ORC_NSPECTV];
+    double qexti[ORC_NSPECTI], qscati[ORC_NSPECTI], gi[ORC_NSPECTI];
+    double gweight[ORC_NGAUSS];
+    double wrefh2o[ORC_REFH2O];
+} orc_tables;
+
+/* Raw k-coefficient records as stored in the reference data files
+ * (CO2H2O_V_12_95_INTEL, CO2H2O_IR_12_95_INTEL), before laginterp. */
+int orc_read_ktables(const char *vis_path, const char *ir_path,
+                     double *co2v8, double *fzerov, double *co2i8, double *fzeroi);
+
+/* Build every table from raw k records (setspv, setspi, setrad/laginterp). */
+void orc_build_tables(orc_tables *t, const double *co2v8, const double *fzerov,
+                      const double *co2i8, const double *fzeroi);
+
+/* Convenience: read + build.  Returns 0 or a negative error. */
+int orc_tables_load(orc_tables *t, const char *vis_path, const char *ir_path);
+
+size_t orc_tables_size(void);
+
+/* tpindex.f90 restated: bins (1-based, as in Fortran) and weights. */
+void orc_tpindex(const orc_tables *t, double pw, double tw, double qh2o,
+                 double lcoef[4], int *mt, int *mp, int *nh2o, double *wratio);
+
+typedef struct {
+    int ncol, L;
+    /* inputs */
+    const double *plev, *tlev, *pmid, *tmid, *qh2o;
+    const double *tauref, *qextrefdst, *taurefcld, *qextrefcld;
+    const double *qxvdst, *qsvdst, *gvdst, *qxidst, *qsidst, *gidst;
+    const double *qxvcld, *qsvcld, *gvcld, *qxicld, *qsicld, *gicld; /* may be NULL */
+    const double *acosz, *als, *albi, *pcol;
+    const double *sol;   /* [7] */
+    const double *sigma; /* [2L+3] */
+    double ptrop;
+    /* in/out */
+    double *detau, *cumtauv;
+    /* outputs */
+    double *fmnetv, *fluxupv, *fluxdnv, *fmneti, *fluxupi, *fluxdni;
+    double *suntot, *irtotal, *qrad;
+    double *nfluxtopv, *nfluxtopi, *diffvt;
+    double *dnvflux, *dndiffv, *dnirflux, *fluxsurf;
+} orc_batch;
+
+/* Full radiation block for every column of the batch; nthreads<=0 uses
+ * all online cores (pthreads).  Returns 0 or a negative error. */
+int orc_run_batch(const orc_tables *t, const orc_batch *b, int nthreads);
+
+/* Debug access to the optical depths of one column (optcv/optci outputs).
+ * dtauv [7][17][L+1], taucumv [7][17][2L+3], taugsurf [7][16] etc. */
+void orc_optics_column(const orc_tables *t, const orc_batch *b, int col,
+                       double *dtauv, double *wbarv, double *cosbv, double *taucumv,
+                       double *taugsurfv, double *dtaui, double *wbari, double *cosbi,
+                       double *taucumi, double *taugsurfi);
+
+/* dsolflux.f: direct-beam surface flux from DETAU, per column. */
+void orc_dsolflux(const orc_tables *t, int ncol, const double *sol, const double *acosz,
+                  const double *detau, double *directsol);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

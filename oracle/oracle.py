@@ -1,0 +1,179 @@
+"""ctypes wrapper of the CPU oracle (TEST INFRASTRUCTURE ONLY).
+
+Only tests/, __graft_entry__.smoke() and bench.py (the cpu_baseline leg and
+the reference arm) import this module, always as the checker.  The product
+library never calls it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import pathlib
+import subprocess
+
+import numpy as np
+
+HERE = pathlib.Path(__file__).resolve().parent
+LIB = HERE / "_build" / "liboracle.so"
+
+NTAB_V = 7 * 51 * 10 * 7 * 17
+NTAB_I = 7 * 51 * 10 * 5 * 17
+NRAW_V = 7 * 11 * 10 * 7 * 17
+NRAW_I = 7 * 11 * 10 * 5 * 17
+
+_D = C.POINTER(C.c_double)
+
+
+class OrcBatch(C.Structure):
+    _fields_ = [("ncol", C.c_int), ("L", C.c_int)] + [
+        (n, _D) for n in (
+            "plev", "tlev", "pmid", "tmid", "qh2o",
+            "tauref", "qextrefdst", "taurefcld", "qextrefcld",
+            "qxvdst", "qsvdst", "gvdst", "qxidst", "qsidst", "gidst",
+            "qxvcld", "qsvcld", "gvcld", "qxicld", "qsicld", "gicld",
+            "acosz", "als", "albi", "pcol", "sol", "sigma")
+    ] + [("ptrop", C.c_double)] + [
+        (n, _D) for n in (
+            "detau", "cumtauv",
+            "fmnetv", "fluxupv", "fluxdnv", "fmneti", "fluxupi", "fluxdni",
+            "suntot", "irtotal", "qrad",
+            "nfluxtopv", "nfluxtopi", "diffvt", "dnvflux", "dndiffv", "dnirflux", "fluxsurf")
+    ]
+
+
+def build() -> pathlib.Path:
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    return LIB
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not LIB.exists():
+            build()
+        _lib = C.CDLL(str(LIB))
+        _lib.orc_tables_size.restype = C.c_size_t
+        _lib.orc_tables_load.argtypes = [C.c_void_p, C.c_char_p, C.c_char_p]
+        _lib.orc_read_ktables.argtypes = [C.c_char_p, C.c_char_p, _D, _D, _D, _D]
+        _lib.orc_build_tables.argtypes = [C.c_void_p, _D, _D, _D, _D]
+        _lib.orc_run_batch.argtypes = [C.c_void_p, C.POINTER(OrcBatch), C.c_int]
+        _lib.orc_tpindex.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double, _D,
+                                     C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                     C.POINTER(C.c_int), _D]
+        _lib.orc_optics_column.argtypes = [C.c_void_p, C.POINTER(OrcBatch), C.c_int] + [_D] * 10
+        _lib.orc_dsolflux.argtypes = [C.c_void_p, C.c_int, _D, _D, _D, _D]
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data_as(_D) if a is not None else None
+
+
+class Tables:
+    """orc_tables built from the two k-coefficient files of a data directory."""
+
+    OFFSETS = None
+
+    def __init__(self, data_dir):
+        L = lib()
+        self.buf = np.zeros(L.orc_tables_size() // 8, dtype=np.float64)
+        d = pathlib.Path(data_dir)
+        rc = L.orc_tables_load(self.buf.ctypes.data, str(d / "CO2H2O_V_12_95_INTEL").encode(),
+                               str(d / "CO2H2O_IR_12_95_INTEL").encode())
+        if rc != 0:
+            raise RuntimeError(f"oracle table load failed ({rc}) from {d}")
+
+    @property
+    def ptr(self):
+        return self.buf.ctypes.data
+
+    def view(self):
+        """Named views into the table struct (layout of orc_tables)."""
+        sizes = [("co2v", NTAB_V), ("co2i", NTAB_I), ("fzerov", 7), ("fzeroi", 5),
+                 ("pfgasref", 51), ("tgasref", 7), ("pgasref", 11), ("planckir", 5 * 8501),
+                 ("wnov", 7), ("dwnv", 7), ("wavev", 7), ("solarf", 7), ("tauray", 7),
+                 ("wnoi", 5), ("dwni", 5), ("wavei", 5), ("qextv", 7), ("qscatv", 7), ("gv", 7),
+                 ("qexti", 5), ("qscati", 5), ("gi", 5), ("gweight", 17), ("wrefh2o", 10)]
+        out, o = {}, 0
+        for n, s in sizes:
+            out[n] = self.buf[o:o + s]
+            o += s
+        return out
+
+    def tpindex(self, pw, tw, qh2o):
+        lc = np.zeros(4)
+        mt, mp, nh = C.c_int(), C.c_int(), C.c_int()
+        wr = np.zeros(1)
+        lib().orc_tpindex(self.ptr, pw, tw, qh2o, _p(lc), C.byref(mt), C.byref(mp),
+                          C.byref(nh), _p(wr))
+        return mt.value, mp.value, nh.value, float(wr[0]), lc
+
+
+def _contig(b, k):
+    v = b.get(k)
+    return None if v is None else np.ascontiguousarray(v, dtype=np.float64)
+
+
+def make_struct(b: dict, out: dict) -> tuple[OrcBatch, list]:
+    keep = []
+    s = OrcBatch()
+    s.ncol = int(b["ncol"])
+    s.L = int(b["L"])
+    for n in ("plev", "tlev", "pmid", "tmid", "qh2o", "tauref", "qextrefdst", "taurefcld",
+              "qextrefcld", "qxvdst", "qsvdst", "gvdst", "qxidst", "qsidst", "gidst", "qxvcld",
+              "qsvcld", "gvcld", "qxicld", "qsicld", "gicld", "acosz", "als", "albi", "pcol",
+              "sol", "sigma"):
+        a = _contig(b, n)
+        keep.append(a)
+        setattr(s, n, _p(a))
+    s.ptrop = float(b["ptrop"])
+    for n in out:
+        setattr(s, n, _p(out[n]))
+    return s, keep
+
+
+def alloc_outputs(ncol: int, L: int, detau=None, cumtauv=None) -> dict:
+    nl = L + 1
+    out = {n: np.zeros((ncol, nl)) for n in (
+        "fmnetv", "fluxupv", "fluxdnv", "fmneti", "fluxupi", "fluxdni", "suntot", "irtotal", "qrad")}
+    for n in ("nfluxtopv", "nfluxtopi", "diffvt", "dnvflux", "dndiffv", "dnirflux", "fluxsurf"):
+        out[n] = np.zeros(ncol)
+    out["detau"] = np.array(detau, dtype=np.float64, copy=True) if detau is not None else np.zeros((ncol, 17, 7))
+    out["cumtauv"] = (np.array(cumtauv, dtype=np.float64, copy=True) if cumtauv is not None
+                      else np.zeros((ncol, 17, 7)))
+    return out
+
+
+def run_batch(tables: Tables, b: dict, nthreads: int = 0) -> dict:
+    out = alloc_outputs(int(b["ncol"]), int(b["L"]), b.get("detau"), b.get("cumtauv"))
+    s, keep = make_struct(b, out)
+    rc = lib().orc_run_batch(tables.ptr, C.byref(s), nthreads)
+    if rc != 0:
+        raise RuntimeError(f"oracle run failed ({rc})")
+    return out
+
+
+def optics_column(tables: Tables, b: dict, col: int) -> dict:
+    L = int(b["L"])
+    nl, lev = L + 1, 2 * L + 3
+    r = {"dtauv": np.zeros((17, 7, nl)), "wbarv": np.zeros((17, 7, nl)), "cosbv": np.zeros((17, 7, nl)),
+         "taucumv": np.zeros((17, 7, lev)), "taugsurfv": np.zeros((16, 7)),
+         "dtaui": np.zeros((17, 5, nl)), "wbari": np.zeros((17, 5, nl)), "cosbi": np.zeros((17, 5, nl)),
+         "taucumi": np.zeros((17, 5, lev)), "taugsurfi": np.zeros((16, 5))}
+    out = alloc_outputs(int(b["ncol"]), L)
+    s, keep = make_struct(b, out)
+    lib().orc_optics_column(tables.ptr, C.byref(s), col, *[_p(r[k]) for k in (
+        "dtauv", "wbarv", "cosbv", "taucumv", "taugsurfv", "dtaui", "wbari", "cosbi", "taucumi",
+        "taugsurfi")])
+    return r
+
+
+def dsolflux(tables: Tables, sol, acosz, detau) -> np.ndarray:
+    acosz = np.ascontiguousarray(acosz, dtype=np.float64)
+    detau = np.ascontiguousarray(detau, dtype=np.float64)
+    sol = np.ascontiguousarray(sol, dtype=np.float64)
+    out = np.zeros(acosz.shape[0])
+    lib().orc_dsolflux(tables.ptr, acosz.shape[0], _p(sol), _p(acosz), _p(detau), _p(out))
+    return out

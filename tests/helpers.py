@@ -1,0 +1,65 @@
+"""Comparison helpers for the parity tests."""
+import numpy as np
+
+from mgcm_rt import OUTPUT_COL, OUTPUT_LAY
+
+FLUX_LAY = ("fmnetv", "fluxupv", "fluxdnv", "fmneti", "fluxupi", "fluxdni")
+DIV_LAY = ("suntot", "irtotal")
+CP, GRAV, KAPA = 735.94, 3.72, 0.25684
+
+
+def flux_scale(ref):
+    """Per-column flux magnitude: largest |flux| of the column (W/m^2)."""
+    s = np.zeros(ref["fluxupi"].shape[0])
+    for k in FLUX_LAY:
+        s = np.maximum(s, np.abs(ref[k]).max(axis=1))
+    return s
+
+
+def heating_scale(b, ref):
+    """Per-layer K/s that one W/m^2 of flux-divergence error makes in QRAD."""
+    plev = np.asarray(b["plev"])
+    L = int(b["L"])
+    nl = L + 1
+    lev = 2 * L + 3
+    ym = np.empty((plev.shape[0], nl))
+    om = np.empty_like(ym)
+    for l in range(1, nl + 1):
+        k = 2 * l
+        ym[:, l - 1] = (float(b["ptrop"]) * 100.0 / GRAV if k == 2
+                        else (plev[:, k] - plev[:, k - 2]) * 100.0 / GRAV)
+        om[:, l - 1] = (plev[:, k - 1] / plev[:, lev - 1]) ** KAPA
+    return 1.0 / (CP * ym * om)
+
+
+def compare(b, got, ref, rtol):
+    """Max error per output, normalised:
+    fluxes:    |d| / (|ref| + rtol-floor at the column's flux scale)
+    SUNTOT/IRTOTAL, scalars: |d| / column flux scale
+    QRAD:      |d| / (column flux scale * heating scale)
+    Returns dict name -> max normalised error (pass when <= rtol)."""
+    fs = flux_scale(ref)[:, None]
+    hs = heating_scale(b, ref)
+    err = {}
+    for k in FLUX_LAY:
+        d = np.abs(np.asarray(got[k]) - ref[k])
+        err[k] = float((d / (np.abs(ref[k]) + fs * 1e-3 + 1e-300)).max()) if d.size else 0.0
+    for k in DIV_LAY:
+        d = np.abs(np.asarray(got[k]) - ref[k])
+        err[k] = float((d / (fs + 1e-300)).max()) if d.size else 0.0
+    d = np.abs(np.asarray(got["qrad"]) - ref["qrad"])
+    err["qrad"] = float((d / (fs * hs + 1e-300)).max()) if d.size else 0.0
+    for k in OUTPUT_COL:
+        d = np.abs(np.asarray(got[k]) - ref[k])
+        err[k] = float((d / (fs[:, 0] + 1e-300)).max()) if d.size else 0.0
+    for k in ("detau", "cumtauv"):
+        d = np.abs(np.asarray(got[k]) - ref[k])
+        err[k] = float((d / (np.abs(ref[k]) + 1e-300)).max()) if d.size else 0.0
+    return err
+
+
+def to_numpy(o):
+    out = {}
+    for k, v in o.items():
+        out[k] = v.detach().cpu().numpy() if hasattr(v, "detach") else np.asarray(v)
+    return out
