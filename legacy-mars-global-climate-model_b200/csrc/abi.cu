@@ -24,7 +24,7 @@ namespace mgcm {
 __global__ void rt_fp64_kernel(const SegTable *__restrict__ st, const double *__restrict__ kv,
                                const double *__restrict__ ki, const double *__restrict__ planck,
                                const RtConst K, int max_nl, uint32_t *status,
-                               unsigned long long *nsys);
+                               unsigned long long *nsys, double *red_scratch);
 __global__ void rt_dsolflux_kernel(int ncol, const double *__restrict__ sol,
                                    const double *__restrict__ acosz,
                                    const double *__restrict__ detau,
@@ -118,6 +118,7 @@ struct mgcm_rt_handle {
     SegTable *d_segs = nullptr;
     SegTable *h_segs = nullptr;   // pinned
     Arena stage;                  // host-pointer staging
+    Arena red;                    // flux staging for L too large for shared memory
     std::mutex mu;
     mgcm_rt_stats stats{};
     size_t budget = 0;
@@ -266,9 +267,11 @@ void fill_direct(SegDev &sd, const mgcm_rt_batch_in &in, const mgcm_rt_batch_out
     sd.fluxsurf = out.fluxsurf;
 }
 
+bool red_in_smem(int max_nl) { return col_smem_bytes(max_nl, true) <= SMEM_CAP; }
+
 int fp64_blocks_per_sm(int max_nl) {
     int nb = 0;
-    const size_t smem = col_smem_bytes(max_nl);
+    const size_t smem = col_smem_bytes(max_nl, red_in_smem(max_nl));
     cudaFuncSetAttribute(rt_fp64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, rt_fp64_kernel, BLOCK, smem) != cudaSuccess)
         return 1;
@@ -287,10 +290,26 @@ int launch_all(mgcm_rt_handle *h, int total, int max_nl, bool validate) {
     }
     CK(cudaEventRecord(h->ev0, h->stream));
     {
-        const size_t smem = col_smem_bytes(max_nl);
+        const bool in_smem = red_in_smem(max_nl);
+        const size_t smem = col_smem_bytes(max_nl, in_smem);
         const int grid = std::min(total, h->num_sms * fp64_blocks_per_sm(max_nl));
+        double *red = nullptr;
+        if (!in_smem) {
+            const size_t need = (size_t)grid * red_bytes(max_nl);
+            if (h->red.bytes < need) {
+                if (h->red.ptr) {
+                    CK(cudaStreamSynchronize(h->stream));
+                    cudaFree(h->red.ptr);
+                }
+                h->red.ptr = nullptr;
+                h->red.bytes = 0;
+                if (cudaMalloc(&h->red.ptr, need) != cudaSuccess) return MGCM_RT_ENOMEM;
+                h->red.bytes = need;
+            }
+            red = static_cast<double *>(h->red.ptr);
+        }
         rt_fp64_kernel<<<grid, BLOCK, smem, h->stream>>>(h->d_segs, h->d_kv, h->d_ki, h->d_planck,
-                                                         h->K, max_nl, h->d_status, h->d_nsys);
+                                                         h->K, max_nl, h->d_status, h->d_nsys, red);
     }
     ++nk;
     CK(cudaGetLastError());
@@ -529,6 +548,7 @@ void mgcm_rt_destroy(mgcm_rt_handle *h) {
     cudaFree(h->d_segs);
     if (h->h_segs) cudaFreeHost(h->h_segs);
     if (h->stage.ptr) cudaFree(h->stage.ptr);
+    if (h->red.ptr) cudaFree(h->red.ptr);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
     if (h->own_stream) cudaStreamDestroy(h->own_stream);

@@ -2,6 +2,7 @@
 // per-band aerosol/Rayleigh opacities and the per-layer scattering sums.
 #pragma once
 #include "rt_common.cuh"
+#include "../../include/mgcm_rt_math.h"
 
 namespace mgcm {
 
@@ -39,7 +40,15 @@ struct ColSmem {
     int day;
 };
 
-__host__ __device__ inline size_t col_smem_bytes(int nl) {
+// Largest dynamic shared memory a CTA may use (227 KB opt-in on sm_100).
+constexpr size_t SMEM_CAP = 227 * 1024;
+
+// Bytes of the per-system flux staging (FMIDP/FMIDM for every system).
+__host__ __device__ inline size_t red_bytes(int nl) { return 2 * (size_t)NSYS * nl * sizeof(double); }
+
+// Shared memory of one column.  With red_in_smem false the flux staging
+// lives in a global scratch slab per CTA instead (large L).
+__host__ __device__ inline size_t col_smem_bytes(int nl, bool red_in_smem = true) {
     const size_t lev1 = 2 * nl + 3;   // 1-based k up to LEV+1 = 2L+4 = 2NL+2
     size_t b = 0;
     b += 3 * (lev1 + 1) * sizeof(int);
@@ -47,14 +56,14 @@ __host__ __device__ inline size_t col_smem_bytes(int nl) {
     b += (lev1 + 1) * (D_NV + 2 * D_NI) * sizeof(double);
     b += (nl + 1) * (2 * D_NV + 4 * D_NI) * sizeof(double);
     b += 2 * D_NI * sizeof(double);
-    b += 2 * (size_t)NSYS * nl * sizeof(double);
+    if (red_in_smem) b += red_bytes(nl);
     b += 3 * NSYS * sizeof(double);
     b += 2 * (nl + 1) * sizeof(double) + 4 * sizeof(double);
     b += NSYS + 64;
     return b;
 }
 
-__device__ inline ColSmem carve_smem(unsigned char *base, int nl) {
+__device__ inline ColSmem carve_smem(unsigned char *base, int nl, double *red_global = nullptr) {
     ColSmem s;
     const int lev1 = 2 * nl + 3;
     double *d = reinterpret_cast<double *>(base);
@@ -77,8 +86,13 @@ __device__ inline ColSmem carve_smem(unsigned char *base, int nl) {
     s.pdif_i = take((nl + 1) * D_NI);
     s.bsurf_i = take(D_NI);
     s.pltop_i = take(D_NI);
-    s.fmp = take((size_t)NSYS * nl);
-    s.fmm = take((size_t)NSYS * nl);
+    if (red_global) {
+        s.fmp = red_global;
+        s.fmm = red_global + (size_t)NSYS * nl;
+    } else {
+        s.fmp = take((size_t)NSYS * nl);
+        s.fmm = take((size_t)NSYS * nl);
+    }
     s.sc0 = take(NSYS);
     s.sc1 = take(NSYS);
     s.sc2 = take(NSYS);
@@ -108,7 +122,7 @@ __device__ __forceinline__ int planck_index(double t, uint32_t *status) {
 
 // tpindex (code/tpindex.f90:72-134).  The log10 bin search is done on the
 // pressure against host-computed limits so bins agree bit-for-bit with the
-// host libm; the weight T uses the device log10.
+// host libm; the weight T uses mgcm_rt_log10, bit-identical to the oracle's.
 __device__ __forceinline__ void tpindex_dev(const RtConst &c, double pw, double tw, double qh2o,
                                             int &mt, int &mp, int &nh, double &wratio,
                                             double lk[4]) {
@@ -125,7 +139,7 @@ __device__ __forceinline__ void tpindex_dev(const RtConst &c, double pw, double 
     mp = D_NP - 1;
     for (int n = 2; n <= D_NP - 1; ++n)
         if (pw <= c.plimit[n - 1]) { mp = n - 1; break; }
-    const double pwl = log10(pw);
+    const double pwl = mgcm_rt_log10(pw);
     const double tt = (pwl - c.pfgasref[mp - 1]) / (c.pfgasref[mp] - c.pfgasref[mp - 1]);
     lk[0] = (1.0 - tt) * (1.0 - uu);
     lk[1] = tt * (1.0 - uu);

@@ -23,8 +23,11 @@
 // (code/comp3.f:677-681,735-738,765-771).
 //
 // Built with --fmad=false: like the reference's x86-64 build, no multiply-add
-// is contracted, so every operation rounds as the Fortran does.
+// is contracted, so every operation rounds as the Fortran does.  Every
+// exponential goes through mgcm_rt_exp (include/mgcm_rt_math.h), the routine
+// the CPU oracle uses too, so host and device agree bit-for-bit.
 #include "rt_stage.cuh"
+#include "../../include/mgcm_rt_math.h"
 
 namespace mgcm {
 
@@ -187,7 +190,7 @@ __device__ void solve_vis(const SegDev &sg, int c, int nw, int ng, int sidx, Col
     const double u0 = sg.acosz[c], rsf = sg.als[c], f0pi = sg.sol[nw - 1];
     const double rcp_u0 = 1.0 / u0, rcp_u02 = 1.0 / (u0 * u0);
     const double s3 = (double)sqrtf(3.0f), s3h = (double)(sqrtf(3.0f) * 0.5f);
-    const double bsurf = rsf * u0 * sg.sol[nw - 1] * exp(-dmin(detau / u0, MAXEXP));
+    const double bsurf = rsf * u0 * sg.sol[nw - 1] * mgcm_rt_exp(-dmin(detau / u0, MAXEXP));
     const double btop = 0.0;
     // c0 = LAMDA, c1 = GAMA, c2 = AM, c3 = AP
     auto coef = [&](int l, double et_top, double et_bot) {
@@ -211,7 +214,7 @@ __device__ void solve_vis(const SegDev &sg, int c, int nw, int ng, int sidx, Col
         y.cmm1 = am * et_top;
         y.cp = ap * et_bot;
         y.cm = am * et_bot;
-        const double ep = exp(dmin(TAUMAX, lam * w.a2[l]));
+        const double ep = mgcm_rt_exp(dmin(TAUMAX, lam * w.a2[l]));
         const double em = 1.0 / ep;
         y.e1 = ep + y.gama * em;
         y.e2 = ep - y.gama * em;
@@ -219,13 +222,13 @@ __device__ void solve_vis(const SegDev &sg, int c, int nw, int ng, int sidx, Col
         y.e4 = y.gama * ep - em;
         return y;
     };
-    double et_bot = exp(-dmin(w.a3[NL + 1] / u0, MAXEXP));
-    double et_top = exp(-dmin(w.a3[NL] / u0, MAXEXP));
+    double et_bot = mgcm_rt_exp(-dmin(w.a3[NL + 1] / u0, MAXEXP));
+    double et_top = mgcm_rt_exp(-dmin(w.a3[NL] / u0, MAXEXP));
     Lay hi = coef(NL, et_top, et_bot);
     bottom_row(hi, NL, bsurf, rsf, w);
     for (int n = NL - 1; n >= 1; --n) {
         et_bot = et_top;
-        et_top = exp(-dmin(w.a3[n] / u0, MAXEXP));
+        et_top = mgcm_rt_exp(-dmin(w.a3[n] / u0, MAXEXP));
         const Lay lo = coef(n, et_top, et_bot);
         elim_pair(lo, hi, n, w);
         hi = lo;
@@ -246,24 +249,24 @@ __device__ void solve_vis(const SegDev &sg, int c, int nw, int ng, int sidx, Col
             const double ep = 1.0, em = 1.0;
             const double fup = xk1 * ep + gama * xk2 * em + ap;
             double fdn = xk1 * ep * gama + xk2 * em + am;
-            fdn = fdn + u0 * f0pi * exp(-dmin(0.0 / u0, MAXEXP));
+            fdn = fdn + u0 * f0pi * mgcm_rt_exp(-dmin(0.0 / u0, MAXEXP));
             s.sc0[sidx] = fup;
             s.sc1[sidx] = fdn;
         }
         if (n < NL) {
             const double tcE = n == 1 ? tcE1 : w.a3[n];
-            const double ep = exp(dmin(TAUMAX, lam * (w.a4[n] - tcE)));
+            const double ep = mgcm_rt_exp(dmin(TAUMAX, lam * (w.a4[n] - tcE)));
             const double em = 1.0 / ep;
-            const double et = exp(-dmin(w.a4[n] / u0, MAXEXP));
+            const double et = mgcm_rt_exp(-dmin(w.a4[n] / u0, MAXEXP));
             const double cpmid = ap * et, cmmid = am * et;
             fmp[n - 1] = xk1 * ep + gama * xk2 * em + cpmid;
             double m = xk1 * ep * gama + xk2 * em + cmmid;
             fmm[n - 1] = m + u0 * f0pi * et;
         } else {
-            const double ep = exp(dmin(TAUMAX, lam * (w.a3[NL + 1] - w.a3[NL])));
+            const double ep = mgcm_rt_exp(dmin(TAUMAX, lam * (w.a3[NL + 1] - w.a3[NL])));
             const double em = 1.0 / ep;
             const double taumid = dmin(w.a3[NL + 1], TAUMAX);
-            const double et = exp(-dmin(taumid / u0, MAXEXP));
+            const double et = mgcm_rt_exp(-dmin(taumid / u0, MAXEXP));
             const double cpmid = ap * et, cmmid = am * et;
             fmp[n - 1] = xk1 * ep + gama * xk2 * em + cpmid;
             const double m = xk1 * ep * gama + xk2 * em + cmmid;
@@ -332,7 +335,7 @@ __device__ void solve_ir(const SegDev &sg, int c, int nw, int ng, int sidx, ColS
     const double *plev = sg.plev + (size_t)c * LEV;
     const double rsf = sg.albi[c];
     const double tautop = w.a2[1] * plev[2 - 1] / (plev[4 - 1] - plev[2 - 1]);
-    const double btop = (1.0 - exp(-tautop / UBARI)) * s.pltop_i[nw - 1];
+    const double btop = (1.0 - mgcm_rt_exp(-tautop / UBARI)) * s.pltop_i[nw - 1];
     const double bsurf = s.bsurf_i[nw - 1];
     // c0 = LAMDA, c1 = GAMA, c2 = B1, c3 = TERM
     auto coef = [&](int l) {
@@ -348,7 +351,7 @@ __device__ void solve_ir(const SegDev &sg, int c, int nw, int ng, int sidx, ColS
         y.cm = b0 + b1 * dt - b1 * term;
         y.cpm1 = b0 + b1 * term;
         y.cmm1 = b0 - b1 * term;
-        const double ep = exp(dmin(lam * dt, TAUMAX));
+        const double ep = mgcm_rt_exp(dmin(lam * dt, TAUMAX));
         const double em = 1.0 / ep;
         y.e1 = ep + y.gama * em;
         y.e2 = ep - y.gama * em;
@@ -380,7 +383,7 @@ __device__ void solve_ir(const SegDev &sg, int c, int nw, int ng, int sidx, ColS
         const double lam = w.c0[n], gama = w.c1[n], b1 = w.c2[n], term = w.c3[n];
         const double b0 = s.b0_i[n * D_NI + nw - 1];
         const double dtk = n < NL ? w.a4[n] : w.a2[n];
-        const double ep = exp(dmin(lam * dtk, TAUMAX));
+        const double ep = mgcm_rt_exp(dmin(lam * dtk, TAUMAX));
         const double em = 1.0 / ep;
         const double cpmid = b0 + b1 * dtk + b1 * term;
         const double cmmid = b0 + b1 * dtk - b1 * term;
@@ -440,9 +443,11 @@ __device__ double reduce_family(const ColSmem &s, const RtConst &K, bool vis, in
 __global__ void __launch_bounds__(224, 2)
 rt_fp64_kernel(const SegTable *__restrict__ st, const double *__restrict__ kv,
                const double *__restrict__ ki, const double *__restrict__ planck,
-               const RtConst K, int max_nl, uint32_t *status, unsigned long long *nsys) {
+               const RtConst K, int max_nl, uint32_t *status, unsigned long long *nsys,
+               double *red_scratch) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    ColSmem s = carve_smem(smem_raw, max_nl);
+    ColSmem s = carve_smem(smem_raw, max_nl,
+                           red_scratch ? red_scratch + (size_t)blockIdx.x * 2 * NSYS * max_nl : nullptr);
     SysLocal w;
     unsigned int nsolved = 0;
     const int total = st->total_cols;
@@ -532,10 +537,10 @@ __global__ void rt_dsolflux_kernel(int ncol, const double *__restrict__ sol,
             const double factor = u0 * sol[nw - 1];
             for (int ng = 1; ng <= D_NG - 1; ++ng) {
                 const double d = de[(nw - 1) + 7 * (ng - 1)];
-                if (d <= 5.0) ds = ds + factor * exp(-d / u0) * K.gweight[ng - 1] * (1.0 - K.fzerov[nw - 1]);
+                if (d <= 5.0) ds = ds + factor * mgcm_rt_exp(-d / u0) * K.gweight[ng - 1] * (1.0 - K.fzerov[nw - 1]);
             }
             const double d = de[(nw - 1) + 7 * 16];
-            if (d <= 5.0) ds = ds + factor * exp(-d / u0) * K.fzerov[nw - 1];
+            if (d <= 5.0) ds = ds + factor * mgcm_rt_exp(-d / u0) * K.fzerov[nw - 1];
         }
     }
     dnvflux[c] = dndiffv[c] + ds;

@@ -14,9 +14,8 @@
  *     addition-chain expansion of constant integer powers);
  *   - real-to-integer assignment truncates toward zero.
  *
- * Parity status: this restatement is pinned against the reference Fortran
- * itself by tests/golden (fixtures produced by executing the reference
- * source files; see tests/golden/make_golden.py).
+ * Exponentials inside a column use the deterministic routine of
+ * include/mgcm_rt_math.h (build with -DORC_LIBM_EXP for the host libm).
  */
 #include "mgcm_rt_oracle.h"
 
@@ -29,6 +28,18 @@
 #include <unistd.h>
 
 #define R4(x) ((double)(float)(x))
+
+/* Per-column exponentials use the shared deterministic exp so the oracle and
+ * the FP64 device path agree bit-for-bit (see include/mgcm_rt_math.h for why
+ * the reference IR solver needs this).  Built with -DORC_LIBM_EXP the oracle
+ * calls the host libm exp instead, which measures the libm sensitivity of the
+ * reference algorithm.  Table set-up (Planck integrals) always uses libm. */
+#include "../include/mgcm_rt_math.h"
+#ifdef ORC_LIBM_EXP
+#define cexp_(x) exp(x)
+#else
+#define cexp_(x) mgcm_rt_exp(x)
+#endif
 
 /* constants_h (code/modules.f90:118-148) */
 static const double PI = 3.1415926535897932;
@@ -284,6 +295,9 @@ void orc_tpindex(const orc_tables *t, double pw, double tw, double qh2o, double 
             }
     }
     double u = (tw - tref[mt - 1]) / (tref[mt] - tref[mt - 1]);
+    /* bins from the host libm LOG10 (as the reference build); the weight
+     * from the shared deterministic log10 (the IR solver amplifies its last
+     * bit by ~1e9, see include/mgcm_rt_math.h) */
     double pwl = log10(pw);
     mp = ORC_PINT - 1;
     for (int n = 2; n <= ORC_PINT - 1; n++)
@@ -291,6 +305,9 @@ void orc_tpindex(const orc_tables *t, double pw, double tw, double qh2o, double 
             mp = n - 1;
             break;
         }
+#ifndef ORC_LIBM_EXP
+    pwl = mgcm_rt_log10(pw);
+#endif
     double tt = (pwl - pref[mp - 1]) / (pref[mp] - pref[mp - 1]);
     lcoef[0] = (1.0 - tt) * (1.0 - u);
     lcoef[1] = tt * (1.0 - u);
@@ -691,8 +708,8 @@ static void gfluxv(int nlay, int lev, double ubar0, double f0pi, double rsf, dou
         double am = f0pi * w0[l] * (g4 * (w->g1[l] + 1.0 / ubar0) + w->g2[l] * w->g3[l]) / denom;
         double ap = f0pi * w0[l] * (w->g3[l] * (w->g1[l] - 1.0 / ubar0) + w->g2[l] * g4) / denom;
         double x0 = tau[l] / ubar0, x1 = tau[l + 1] / ubar0;
-        double et0 = exp(-(x0 < MAXEXP ? x0 : MAXEXP));
-        double et1 = exp(-(x1 < MAXEXP ? x1 : MAXEXP));
+        double et0 = cexp_(-(x0 < MAXEXP ? x0 : MAXEXP));
+        double et1 = cexp_(-(x1 < MAXEXP ? x1 : MAXEXP));
         w->cpm1[l] = ap * et0;
         w->cmm1[l] = am * et0;
         w->cp[l] = ap * et1;
@@ -701,7 +718,7 @@ static void gfluxv(int nlay, int lev, double ubar0, double f0pi, double rsf, dou
     for (int l = 1; l <= nlay; l++) {
         double x = w->lamda[l] * w->dtaul[l];
         double exptrm = TAUMAX < x ? TAUMAX : x;
-        double ep = exp(exptrm);
+        double ep = cexp_(exptrm);
         double em = 1.0 / ep;
         w->e1[l] = ep + w->gama[l] * em;
         w->e2[l] = ep - w->gama[l] * em;
@@ -712,7 +729,7 @@ static void gfluxv(int nlay, int lev, double ubar0, double f0pi, double rsf, dou
     for (int l = 1; l <= nlay - 1; l++) {
         double x = w->lamda[l] * (tcum[2 * l + 1] - tcum[2 * l]);
         double exptrm = TAUMAX < x ? TAUMAX : x;
-        double ep = exp(exptrm);
+        double ep = cexp_(exptrm);
         double em = 1.0 / ep;
         double g4 = 1.0 - w->g3[l];
         double denom = w->lamda[l] * w->lamda[l] - 1.0 / (ubar0 * ubar0);
@@ -721,7 +738,7 @@ static void gfluxv(int nlay, int lev, double ubar0, double f0pi, double rsf, dou
         double ap = f0pi * w0[l] * (w->g3[l] * (w->g1[l] - 1.0 / ubar0) + w->g2[l] * g4) / denom;
         double taumid = tcum[2 * l + 1];
         double xm = taumid / ubar0;
-        double et = exp(-(xm < MAXEXP ? xm : MAXEXP));
+        double et = cexp_(-(xm < MAXEXP ? xm : MAXEXP));
         double cpmid = ap * et;
         double cmmid = am * et;
         w->fmidp[l] = w->xk1[l] * ep + w->gama[l] * w->xk2[l] * em + cpmid;
@@ -739,13 +756,13 @@ static void gfluxv(int nlay, int lev, double ubar0, double f0pi, double rsf, dou
         *fluxup = w->xk1[1] * ep + w->gama[1] * w->xk2[1] * em + cpmid;
         *fluxdn = w->xk1[1] * ep * w->gama[1] + w->xk2[1] * em + cmmid;
         double x = tcum[1] / ubar0;
-        *fluxdn = *fluxdn + ubar0 * f0pi * exp(-(x < MAXEXP ? x : MAXEXP));
+        *fluxdn = *fluxdn + ubar0 * f0pi * cexp_(-(x < MAXEXP ? x : MAXEXP));
     }
     {
         int l = nlay;
         double x = w->lamda[l] * (tcum[lev] - tcum[lev - 1]);
         double exptrm = TAUMAX < x ? TAUMAX : x;
-        double ep = exp(exptrm);
+        double ep = cexp_(exptrm);
         double em = 1.0 / ep;
         double g4 = 1.0 - w->g3[l];
         double denom = w->lamda[l] * w->lamda[l] - 1.0 / (ubar0 * ubar0);
@@ -754,7 +771,7 @@ static void gfluxv(int nlay, int lev, double ubar0, double f0pi, double rsf, dou
         double ap = f0pi * w0[l] * (w->g3[l] * (w->g1[l] - 1.0 / ubar0) + w->g2[l] * g4) / denom;
         double taumid = tcum[lev] < TAUMAX ? tcum[lev] : TAUMAX;
         double xm = taumid / ubar0;
-        double et = exp(-(xm < MAXEXP ? xm : MAXEXP));
+        double et = cexp_(-(xm < MAXEXP ? xm : MAXEXP));
         double cpmid = ap * et;
         double cmmid = am * et;
         w->fmidp[l] = w->xk1[l] * ep + w->gama[l] * w->xk2[l] * em + cpmid;
@@ -795,7 +812,7 @@ static void gfluxi(int nlay, const orc_tables *t, const double *tlev, int nw, co
     }
     for (int l = 1; l <= nlay; l++) {
         double x = w->lamda[l] * dtau[l];
-        double ep = exp(x < TAUMAX ? x : TAUMAX);
+        double ep = cexp_(x < TAUMAX ? x : TAUMAX);
         double em = 1.0 / ep;
         w->e1[l] = ep + w->gama[l] * em;
         w->e2[l] = ep - w->gama[l] * em;
@@ -806,7 +823,7 @@ static void gfluxi(int nlay, const orc_tables *t, const double *tlev, int nw, co
     for (int l = 1; l <= nlay - 1; l++) {
         double dtauk = taucum[2 * l + 1] - taucum[2 * l];
         double x = w->lamda[l] * dtauk;
-        double ep = exp(x < TAUMAX ? x : TAUMAX);
+        double ep = cexp_(x < TAUMAX ? x : TAUMAX);
         double em = 1.0 / ep;
         double term = UBARI / (1.0 - w0[l] * cosbar[l]);
         double cpmid = w->b0[l] + w->b1[l] * dtauk + w->b1[l] * term;
@@ -819,7 +836,7 @@ static void gfluxi(int nlay, const orc_tables *t, const double *tlev, int nw, co
     {
         int l = nlay;
         double x = w->lamda[l] * dtau[l];
-        double ep = exp(x < TAUMAX ? x : TAUMAX);
+        double ep = cexp_(x < TAUMAX ? x : TAUMAX);
         double em = 1.0 / ep;
         double term = UBARI / (1.0 - w0[l] * cosbar[l]);
         double cpmid = w->b0[l] + w->b1[l] * dtau[l] + w->b1[l] * term;
@@ -922,7 +939,7 @@ static void column(const orc_tables *t, const orc_batch *b, int col, work_t *w) 
                 double btop = 0.0;
                 double x = de / ubar0;
                 double eterm = x < MAXEXP ? x : MAXEXP;
-                double bsurf = rsfv * ubar0 * b->sol[nw - 1] * exp(-eterm);
+                double bsurf = rsfv * ubar0 * b->sol[nw - 1] * cexp_(-eterm);
                 double diffv, fluxup, fluxdn;
                 gfluxv(NLAY, LEV, ubar0, f0pi, rsfv, btop, bsurf, w, &diffv, &fluxup, &fluxdn);
                 if (ng < 17) {
@@ -987,7 +1004,7 @@ static void column(const orc_tables *t, const orc_batch *b, int col, work_t *w) 
                 }
                 for (int k = 1; k <= LEV; k++) tci[k] = A3(w->taucum, LEV, 5, k, nw, ng);
                 double tautop = dtau[1] * plev[2 - 1] / (plev[4 - 1] - plev[2 - 1]);
-                double btop = (1.0 - exp(-tautop / UBARI)) * pltop;
+                double btop = (1.0 - cexp_(-tautop / UBARI)) * pltop;
                 double ftopup;
                 gfluxi(NLAY, t, tlev, nw, dtau, tci, wb, cb, albi, btop, bsurf, w, &ftopup);
                 double dw = t->dwni[nw - 1];
@@ -1154,12 +1171,16 @@ void orc_dsolflux(const orc_tables *t, int ncol, const double *sol, const double
                 for (int ng = 1; ng <= 16; ng++) {
                     double d = de[(nw - 1) + 7 * (ng - 1)];
                     if (d <= 5.0)
-                        ds = ds + factor * exp(-d / ubar0) * t->gweight[ng - 1] * (1.0 - t->fzerov[nw - 1]);
+                        ds = ds + factor * cexp_(-d / ubar0) * t->gweight[ng - 1] * (1.0 - t->fzerov[nw - 1]);
                 }
                 double d = de[(nw - 1) + 7 * 16];
-                if (d <= 5.0) ds = ds + factor * exp(-d / ubar0) * t->fzerov[nw - 1];
+                if (d <= 5.0) ds = ds + factor * cexp_(-d / ubar0) * t->fzerov[nw - 1];
             }
         }
         directsol[col] = ds;
     }
 }
+
+/* The column exponential and logarithm, exported for tests. */
+double orc_exp(double x) { return cexp_(x); }
+double orc_log10(double x) { return mgcm_rt_log10(x); }

@@ -14,6 +14,9 @@ import numpy as np
 
 HERE = pathlib.Path(__file__).resolve().parent
 LIB = HERE / "_build" / "liboracle.so"
+# variant "libm": column exponentials from the host libm instead of the shared
+# deterministic exp (measures the reference algorithm's libm sensitivity)
+LIBS = {"rt": LIB, "libm": HERE / "_build" / "liboracle_libm.so"}
 
 NTAB_V = 7 * 51 * 10 * 7 * 17
 NTAB_I = 7 * 51 * 10 * 5 * 17
@@ -45,15 +48,16 @@ def build() -> pathlib.Path:
     return LIB
 
 
-_lib = None
+_libs = {}
 
 
-def lib():
-    global _lib
+def lib(variant: str = "rt"):
+    _lib = _libs.get(variant)
     if _lib is None:
-        if not LIB.exists():
+        path = LIBS[variant]
+        if not path.exists():
             build()
-        _lib = C.CDLL(str(LIB))
+        _lib = C.CDLL(str(path))
         _lib.orc_tables_size.restype = C.c_size_t
         _lib.orc_tables_load.argtypes = [C.c_void_p, C.c_char_p, C.c_char_p]
         _lib.orc_read_ktables.argtypes = [C.c_char_p, C.c_char_p, _D, _D, _D, _D]
@@ -64,6 +68,7 @@ def lib():
                                      C.POINTER(C.c_int), _D]
         _lib.orc_optics_column.argtypes = [C.c_void_p, C.POINTER(OrcBatch), C.c_int] + [_D] * 10
         _lib.orc_dsolflux.argtypes = [C.c_void_p, C.c_int, _D, _D, _D, _D]
+        _libs[variant] = _lib
     return _lib
 
 
@@ -76,8 +81,9 @@ class Tables:
 
     OFFSETS = None
 
-    def __init__(self, data_dir):
-        L = lib()
+    def __init__(self, data_dir, variant: str = "rt"):
+        self.variant = variant
+        L = lib(variant)
         self.buf = np.zeros(L.orc_tables_size() // 8, dtype=np.float64)
         d = pathlib.Path(data_dir)
         rc = L.orc_tables_load(self.buf.ctypes.data, str(d / "CO2H2O_V_12_95_INTEL").encode(),
@@ -106,7 +112,7 @@ class Tables:
         lc = np.zeros(4)
         mt, mp, nh = C.c_int(), C.c_int(), C.c_int()
         wr = np.zeros(1)
-        lib().orc_tpindex(self.ptr, pw, tw, qh2o, _p(lc), C.byref(mt), C.byref(mp),
+        lib(self.variant).orc_tpindex(self.ptr, pw, tw, qh2o, _p(lc), C.byref(mt), C.byref(mp),
                           C.byref(nh), _p(wr))
         return mt.value, mp.value, nh.value, float(wr[0]), lc
 
@@ -149,7 +155,7 @@ def alloc_outputs(ncol: int, L: int, detau=None, cumtauv=None) -> dict:
 def run_batch(tables: Tables, b: dict, nthreads: int = 0) -> dict:
     out = alloc_outputs(int(b["ncol"]), int(b["L"]), b.get("detau"), b.get("cumtauv"))
     s, keep = make_struct(b, out)
-    rc = lib().orc_run_batch(tables.ptr, C.byref(s), nthreads)
+    rc = lib(tables.variant).orc_run_batch(tables.ptr, C.byref(s), nthreads)
     if rc != 0:
         raise RuntimeError(f"oracle run failed ({rc})")
     return out
@@ -164,7 +170,7 @@ def optics_column(tables: Tables, b: dict, col: int) -> dict:
          "taucumi": np.zeros((17, 5, lev)), "taugsurfi": np.zeros((16, 5))}
     out = alloc_outputs(int(b["ncol"]), L)
     s, keep = make_struct(b, out)
-    lib().orc_optics_column(tables.ptr, C.byref(s), col, *[_p(r[k]) for k in (
+    lib(tables.variant).orc_optics_column(tables.ptr, C.byref(s), col, *[_p(r[k]) for k in (
         "dtauv", "wbarv", "cosbv", "taucumv", "taugsurfv", "dtaui", "wbari", "cosbi", "taucumi",
         "taugsurfi")])
     return r
@@ -175,5 +181,5 @@ def dsolflux(tables: Tables, sol, acosz, detau) -> np.ndarray:
     detau = np.ascontiguousarray(detau, dtype=np.float64)
     sol = np.ascontiguousarray(sol, dtype=np.float64)
     out = np.zeros(acosz.shape[0])
-    lib().orc_dsolflux(tables.ptr, acosz.shape[0], _p(sol), _p(acosz), _p(detau), _p(out))
+    lib(tables.variant).orc_dsolflux(tables.ptr, acosz.shape[0], _p(sol), _p(acosz), _p(detau), _p(out))
     return out

@@ -170,3 +170,38 @@ def test_dsolflux_oracle_matches_closed_form(otables):
     w = np.outer(gw[:16].sum() * np.ones(7), 1)[:, 0] * (1 - fz) + fz
     exp = (b["acosz"][:, None] * b["sol"][None, :] * np.exp(-0.3 / b["acosz"][:, None]) * w[None, :]).sum(1)
     np.testing.assert_allclose(ds, exp, rtol=1e-12)
+
+
+def test_libm_sensitivity_of_reference_ir(data_dir, otables):
+    """The reference IR two-stream amplifies one-ulp differences of EXP
+    (EP-EM cancellation in thin layers); visible stays at rounding level.
+    This bounds what any exp implementation can change."""
+    from helpers import compare
+    t2 = oracle.Tables(data_dir, variant="libm")
+    b = synth.make_batch(64, L=24, seed=2, cloud=True)
+    a = oracle.run_batch(otables, b)
+    c = oracle.run_batch(t2, b)
+    err = compare(b, c, a, 1e-12)
+    assert err["fmnetv"] < 1e-11 and err["fluxdnv"] < 1e-11
+    assert err["fmneti"] < 1e-4 and err["fluxupi"] < 1e-4
+    assert 0 < max(err["fmneti"], err["fluxdni"])
+
+
+def test_shared_exp_accuracy():
+    import ctypes
+    L = oracle.lib()
+    m = ctypes.CDLL("libm.so.6")
+    m.exp.restype = ctypes.c_double
+    m.exp.argtypes = [ctypes.c_double]
+    L.orc_exp.restype = ctypes.c_double
+    L.orc_exp.argtypes = [ctypes.c_double]
+    rng = np.random.default_rng(1)
+    xs = np.concatenate([rng.uniform(-40, 40, 20000), rng.uniform(-700, 700, 2000),
+                         [0.0, -35.0, 35.0, 1e-300, -1e-300]])
+    same = 0
+    for x in xs:
+        a, b = L.orc_exp(float(x)), m.exp(float(x))
+        assert abs(a - b) <= math.ulp(b) * 1.0001
+        same += a == b
+    assert same / len(xs) > 0.99
+    assert L.orc_exp(0.0) == 1.0
