@@ -42,6 +42,9 @@ WORKLOADS = {
                name="36x60 = 2,160 columns x 24 layers, dust only, half night"),
     "c4": dict(ncol=1036800 // 8, L=48, cloud=True,
                name="720x1440 x 48 layers, one eighth (129,600 columns) per call"),
+    # profiling case: inputs ~320 MB (> L2) but a small device footprint
+    "prof": dict(ncol=8192, L=24, cloud=True,
+                 name="8,192 columns x 24 layers, dust + water-ice cloud (ncu case)"),
 }
 
 
