@@ -171,6 +171,26 @@ int mgcm_rt_get_stats(mgcm_rt_handle *h, mgcm_rt_stats *st);
 int mgcm_rt_tables_host(const char *data_dir, double *co2v, double *co2i, double *planckir,
                         double *pfgasref);
 
+/* No-allocation run (no counterpart in the reference; the reference has no
+ * device memory at all).  For callers that must not allocate device memory
+ * once they are running: a host whose device memory is owned by another
+ * allocator (a framework's caching pool), a time-stepping loop that forbids
+ * allocation after start-up, a process under a hard device-memory quota.
+ * Tables come from the handle (allocated once by mgcm_rt_create); inputs and
+ * outputs are the caller's device buffers (in->device_ptrs must be set).  The
+ * call itself allocates nothing: its scratch -- the batch descriptor, the
+ * status word and the per-CTA flux staging of the FP64 kernel -- lives in one
+ * file-scope static device array of MGCM_RT_NOALLOC_SCRATCH_BYTES that every
+ * GPU which loads the library holds until exit.  Runs the FP64 kernel on the
+ * handle's stream and waits for it.  Its first call on a device does the
+ * set-up: it resolves the array's device address on that device (once per
+ * device); make that first call before any stream capture begins.  All calls
+ * share the one array, so calls that overlap on the GPU (different threads or
+ * handles on the same device) race; serialise them.  Returns MGCM_RT_EINVAL
+ * for host pointers and MGCM_RT_ENOMEM if one CTA's staging would not fit. */
+#define MGCM_RT_NOALLOC_SCRATCH_BYTES (16u << 20)
+int mgcm_rt_run_noalloc(mgcm_rt_handle *h, const mgcm_rt_batch_in *in, mgcm_rt_batch_out *out);
+
 void mgcm_rt_destroy(mgcm_rt_handle *h);
 const char *mgcm_rt_strerror(int status);
 const char *mgcm_rt_version(void);

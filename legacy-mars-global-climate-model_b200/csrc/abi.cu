@@ -2,6 +2,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstddef>
 #include <atomic>
 #include <chrono>
 #include <cmath>
@@ -673,4 +674,106 @@ int mgcm_rt_wait(mgcm_rt_handle *h, long long ticket, double timeout_s) {
     h->reqs.erase(it);
     return st;
 }
+}
+
+// ---------------------------------------------------------------------------
+// No-allocation entry point.  Its scratch is this file-scope array; in host
+// code the symbol is only a stand-in, so the device address is resolved with
+// cudaGetSymbolAddress once per device (with that device current) and cached.
+namespace {
+
+constexpr size_t NOALLOC_HDR = 64 * 1024;   // descriptor + status + counter
+static_assert(offsetof(SegTable, seg) + sizeof(SegDev) + 512 <= NOALLOC_HDR, "descriptor");
+static_assert(NOALLOC_HDR < MGCM_RT_NOALLOC_SCRATCH_BYTES, "scratch size");
+
+__device__ __align__(256) unsigned char g_noalloc_scratch[MGCM_RT_NOALLOC_SCRATCH_BYTES];
+
+std::mutex g_noalloc_mu;
+unsigned char *g_noalloc_ptr[256] = {};
+
+int noalloc_scratch(int device, unsigned char **ptr) {
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (device < 0 || device >= 256) return MGCM_RT_EINVAL;
+    if (!g_noalloc_ptr[device]) {
+        void *p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return MGCM_RT_ECUDA;
+        g_noalloc_ptr[device] = static_cast<unsigned char *>(p);
+    }
+    *ptr = g_noalloc_ptr[device];
+    return MGCM_RT_OK;
+}
+
+}  // namespace
+
+extern "C" int mgcm_rt_run_noalloc(mgcm_rt_handle *h, const mgcm_rt_batch_in *in,
+                                   mgcm_rt_batch_out *out) {
+    if (!h || !in || !out) return MGCM_RT_EINVAL;
+    if (!in->device_ptrs) return MGCM_RT_EINVAL;   // host buffers would need staging memory
+    std::lock_guard<std::mutex> lk(h->mu);
+    if (cudaSetDevice(h->device) != cudaSuccess) return MGCM_RT_ECUDA;
+    int rc = check_args(h, in, out);
+    if (rc) return rc;
+    if (in->ncol == 0) return MGCM_RT_OK;
+    if (h->pending) {
+        h->pending = false;
+        rc = finish(h, h->pending_cols);
+        if (rc) return rc;
+    }
+    unsigned char *scr = nullptr;
+    rc = noalloc_scratch(h->device, &scr);
+    if (rc) return rc;
+    const Sizes z = sizes_of(*in);
+    const int max_nl = z.nl;
+    // flux staging per CTA in the array; the grid is capped to the slabs that fit
+    const size_t slab = red_bytes(max_nl);
+    const size_t nslab = (MGCM_RT_NOALLOC_SCRATCH_BYTES - NOALLOC_HDR) / slab;
+    if (nslab < 1) return MGCM_RT_ENOMEM;
+    const size_t smem = col_smem_bytes(max_nl, false);
+    if (cudaFuncSetAttribute(rt_fp64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem) != cudaSuccess)
+        return MGCM_RT_ECUDA;
+    int nb = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, rt_fp64_kernel, BLOCK, smem) != cudaSuccess)
+        nb = 1;
+    const size_t want = (size_t)h->num_sms * (size_t)std::max(nb, 1);
+    const int grid = (int)std::min({(size_t)z.ncol, want, nslab});
+    // descriptor: header + one segment, staged through the handle's pinned buffer
+    SegTable &tab = *h->h_segs;
+    tab.nseg = 1;
+    tab.total_cols = (int)z.ncol;
+    SegDev sd{};
+    sd.ncol = (int)z.ncol;
+    sd.L = z.L;
+    sd.col0 = 0;
+    sd.ptrop = in->ptrop;
+    fill_direct(sd, *in, *out);
+    sd.sigma = in->sigma;
+    sd.sol = in->sol;
+    tab.seg[0] = sd;
+    SegTable *d_tab = reinterpret_cast<SegTable *>(scr);
+    uint32_t *d_status = reinterpret_cast<uint32_t *>(scr + NOALLOC_HDR - 256);
+    unsigned long long *d_nsys = reinterpret_cast<unsigned long long *>(scr + NOALLOC_HDR - 128);
+    double *d_red = reinterpret_cast<double *>(scr + NOALLOC_HDR);
+    CK(cudaMemcpyAsync(d_tab, h->h_segs, offsetof(SegTable, seg) + sizeof(SegDev),
+                       cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemsetAsync(d_status, 0, sizeof(uint32_t), h->stream));
+    CK(cudaMemsetAsync(d_nsys, 0, sizeof(unsigned long long), h->stream));
+    CK(cudaEventRecord(h->ev0, h->stream));
+    rt_fp64_kernel<<<grid, BLOCK, smem, h->stream>>>(d_tab, h->d_kv, h->d_ki, h->d_planck, h->K,
+                                                     max_nl, d_status, d_nsys, d_red);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(h->ev1, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    uint32_t st = 0;
+    unsigned long long ns = 0;
+    CK(cudaMemcpy(&st, d_status, sizeof(st), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(&ns, d_nsys, sizeof(ns), cudaMemcpyDeviceToHost));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+    h->stats.gpu_ms = ms;
+    h->stats.columns = (long long)z.ncol;
+    h->stats.systems = (long long)ns;
+    h->stats.status = (int)st;
+    h->stats.kernels = 1;
+    return status_to_code(st);
 }
