@@ -26,6 +26,20 @@ __global__ void rt_fp64_kernel(const SegTable *__restrict__ st, const double *__
                                const double *__restrict__ ki, const double *__restrict__ planck,
                                const RtConst K, int max_nl, uint32_t *status,
                                unsigned long long *nsys, double *red_scratch);
+__global__ void rt_fp64_screen(const SegTable *__restrict__ st, int col_begin, int col_end, int max_nl,
+                               unsigned char *__restrict__ blocks, size_t stride,
+                               const double *__restrict__ kv, const double *__restrict__ ki,
+                               const double *__restrict__ planck, const RtConst K,
+                               int *__restrict__ list_v, int *__restrict__ list_i,
+                               unsigned int *counts, uint32_t *status, unsigned long long *nsys);
+template <bool VIS>
+__global__ void rt_fp64_solve(const SegTable *__restrict__ st, int col_begin, int max_nl,
+                              unsigned char *__restrict__ blocks, size_t stride,
+                              const double *__restrict__ ktab, const RtConst K,
+                              const int *__restrict__ list, const unsigned int *count);
+__global__ void rt_fp64_reduce(const SegTable *__restrict__ st, int col_begin, int col_end,
+                               int max_nl, unsigned char *__restrict__ blocks, size_t stride,
+                               const RtConst K);
 __global__ void rt_dsolflux_kernel(int ncol, const double *__restrict__ sol,
                                    const double *__restrict__ acosz,
                                    const double *__restrict__ detau,
@@ -120,6 +134,8 @@ struct mgcm_rt_handle {
     SegTable *h_segs = nullptr;   // pinned
     Arena stage;                  // host-pointer staging
     Arena red;                    // flux staging for L too large for shared memory
+    Arena pipe;                   // pipeline: per-column blocks, system lists, counters
+    int occ_screen = 0, occ_solve = 0, occ_reduce = 0;
     std::mutex mu;
     mgcm_rt_stats stats{};
     size_t budget = 0;
@@ -279,6 +295,56 @@ int fp64_blocks_per_sm(int max_nl) {
     return std::max(nb, 1);
 }
 
+// Three-kernel FP64 pipeline over chunks of columns (rt_fp64.cu).
+int launch_pipeline(mgcm_rt_handle *h, int total, int max_nl, int &nk) {
+    const size_t stride = (col_smem_bytes(max_nl, true) + 255) / 256 * 256;
+    const size_t per_col = stride + 2 * NSYS * sizeof(int);
+    const size_t cap = std::min<size_t>(h->budget / 2, (size_t)8 << 30);
+    int chunk = (int)std::min<size_t>((size_t)total, std::max<size_t>(cap / per_col, 1));
+    const size_t need = (size_t)chunk * per_col + 256;
+    if (h->pipe.bytes < need) {
+        if (h->pipe.ptr) {
+            CK(cudaStreamSynchronize(h->stream));
+            cudaFree(h->pipe.ptr);
+        }
+        h->pipe.ptr = nullptr;
+        h->pipe.bytes = 0;
+        if (cudaMalloc(&h->pipe.ptr, need) != cudaSuccess) return MGCM_RT_ENOMEM;
+        h->pipe.bytes = need;
+    }
+    unsigned char *blocks = static_cast<unsigned char *>(h->pipe.ptr);
+    int *list_v = reinterpret_cast<int *>(blocks + (size_t)chunk * stride);
+    int *list_i = list_v + (size_t)chunk * NSYS_V;
+    unsigned int *counts = reinterpret_cast<unsigned int *>(list_i + (size_t)chunk * NSYS_I);
+    if (!h->occ_screen) {
+        int a = 1, b = 1, c = 1;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, rt_fp64_screen, BLOCK, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, rt_fp64_solve<false>, 128, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, rt_fp64_reduce, 160, 0);
+        h->occ_screen = std::max(a, 1);
+        h->occ_solve = std::max(b, 1);
+        h->occ_reduce = std::max(c, 1);
+    }
+    for (int c0 = 0; c0 < total; c0 += chunk) {
+        const int c1 = std::min(total, c0 + chunk);
+        CK(cudaMemsetAsync(counts, 0, 2 * sizeof(unsigned int), h->stream));
+        const int g1 = std::min(c1 - c0, h->num_sms * h->occ_screen);
+        rt_fp64_screen<<<g1, BLOCK, 0, h->stream>>>(h->d_segs, c0, c1, max_nl, blocks, stride,
+                                                     h->d_kv, h->d_ki, h->d_planck, h->K, list_v,
+                                                     list_i, counts, h->d_status, h->d_nsys);
+        const int g2 = h->num_sms * h->occ_solve;
+        rt_fp64_solve<true><<<g2, 128, 0, h->stream>>>(h->d_segs, c0, max_nl, blocks, stride,
+                                                        h->d_kv, h->K, list_v, counts);
+        rt_fp64_solve<false><<<g2, 128, 0, h->stream>>>(h->d_segs, c0, max_nl, blocks, stride,
+                                                         h->d_ki, h->K, list_i, counts);
+        const int g3 = std::min(c1 - c0, h->num_sms * h->occ_reduce);
+        rt_fp64_reduce<<<g3, 160, 0, h->stream>>>(h->d_segs, c0, c1, max_nl, blocks, stride, h->K);
+        nk += 4;
+        CK(cudaGetLastError());
+    }
+    return MGCM_RT_OK;
+}
+
 // Launches the radiation kernels for the segment table already in h->d_segs.
 int launch_all(mgcm_rt_handle *h, int total, int max_nl, bool validate) {
     CK(cudaMemsetAsync(h->d_status, 0, sizeof(uint32_t), h->stream));
@@ -290,7 +356,10 @@ int launch_all(mgcm_rt_handle *h, int total, int max_nl, bool validate) {
         ++nk;
     }
     CK(cudaEventRecord(h->ev0, h->stream));
-    {
+    if (h->cfg.precision == MGCM_RT_FP64) {
+        const int rc = launch_pipeline(h, total, max_nl, nk);
+        if (rc) return rc;
+    } else {
         const bool in_smem = red_in_smem(max_nl);
         const size_t smem = col_smem_bytes(max_nl, in_smem);
         const int grid = std::min(total, h->num_sms * fp64_blocks_per_sm(max_nl));
@@ -311,8 +380,8 @@ int launch_all(mgcm_rt_handle *h, int total, int max_nl, bool validate) {
         }
         rt_fp64_kernel<<<grid, BLOCK, smem, h->stream>>>(h->d_segs, h->d_kv, h->d_ki, h->d_planck,
                                                          h->K, max_nl, h->d_status, h->d_nsys, red);
+        ++nk;
     }
-    ++nk;
     CK(cudaGetLastError());
     CK(cudaEventRecord(h->ev1, h->stream));
     h->stats.kernels = nk;
@@ -550,6 +619,7 @@ void mgcm_rt_destroy(mgcm_rt_handle *h) {
     if (h->h_segs) cudaFreeHost(h->h_segs);
     if (h->stage.ptr) cudaFree(h->stage.ptr);
     if (h->red.ptr) cudaFree(h->red.ptr);
+    if (h->pipe.ptr) cudaFree(h->pipe.ptr);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
     if (h->own_stream) cudaStreamDestroy(h->own_stream);

@@ -26,419 +26,12 @@
 // is contracted, so every operation rounds as the Fortran does.  Every
 // exponential goes through mgcm_rt_exp (include/mgcm_rt_math.h), the routine
 // the CPU oracle uses too, so host and device agree bit-for-bit.
-#include "rt_stage.cuh"
+#include "rt_fp64_sys.cuh"
 #include "../../include/mgcm_rt_math.h"
 
 namespace mgcm {
 
-namespace {
-
-constexpr double MAXEXP = 35.0;
-constexpr double TAUMAX = 35.0;
-constexpr double UBARI = 0.5;
-constexpr double PI_D = 3.1415926535897932;
-constexpr double TLIMITS = 1.0e-3;
-constexpr double TLIMITI = 5.0e-3;
-
-struct Lay {   // per-layer two-stream coefficients
-    double gama, e1, e2, e3, e4, cp, cm, cpm1, cmm1;
-};
-
-struct SysLocal {
-    double a0[D_MAXNL + 1], a1[D_MAXNL + 1], a2[D_MAXNL + 1], a3[D_MAXNL + 2], a4[D_MAXNL + 1];
-    double c0[D_MAXNL + 1], c1[D_MAXNL + 1], c2[D_MAXNL + 1], c3[D_MAXNL + 1];
-    double as[2 * D_MAXNL + 1], ds[2 * D_MAXNL + 1];
-};
-
-// One step of the DTRIDGL upward elimination for row i given row i+1's AS/DS.
-__device__ __forceinline__ void elim(double af, double bf, double cf, double df, double as1,
-                                     double ds1, double &as, double &ds) {
-    const double x = 1.0 / (bf - cf * as1);
-    as = af * x;
-    ds = (df - cf * ds1) * x;
-}
-
-// Rows 2n+1 (odd) and 2n (even) of DSOLVER for layers lo = n, hi = n+1.
-__device__ __forceinline__ void elim_pair(const Lay &lo, const Lay &hi, int n, SysLocal &w) {
-    {
-        const int i = 2 * n + 1;
-        const double af = 2.0 * (1.0 - lo.gama * lo.gama);
-        const double bf = (lo.e1 - lo.e3) * (1.0 + hi.gama);
-        const double cf = (lo.e1 + lo.e3) * (hi.gama - 1.0);
-        const double df = lo.e3 * (hi.cpm1 - lo.cp) + lo.e1 * (lo.cm - hi.cmm1);
-        elim(af, bf, cf, df, w.as[i + 1], w.ds[i + 1], w.as[i], w.ds[i]);
-    }
-    {
-        const int i = 2 * n;
-        const double af = (lo.e1 + lo.e3) * (hi.gama - 1.0);
-        const double bf = (lo.e2 + lo.e4) * (hi.gama - 1.0);
-        const double cf = 2.0 * (1.0 - hi.gama * hi.gama);
-        const double df = (hi.gama - 1.0) * (hi.cpm1 - lo.cp) + (1.0 - hi.gama) * (lo.cm - hi.cmm1);
-        elim(af, bf, cf, df, w.as[i + 1], w.ds[i + 1], w.as[i], w.ds[i]);
-    }
-}
-
-__device__ __forceinline__ void bottom_row(const Lay &b, int nl, double bsurf, double rsf,
-                                           SysLocal &w) {
-    const int i = 2 * nl;
-    const double af = b.e1 - rsf * b.e3;
-    const double bf = b.e2 - rsf * b.e4;
-    const double df = bsurf - b.cp + rsf * b.cm;
-    w.as[i] = af / bf;
-    w.ds[i] = df / bf;
-}
-
-__device__ __forceinline__ void top_row(const Lay &t, double btop, SysLocal &w) {
-    const double af = 0.0, bf = t.gama + 1.0, cf = t.gama - 1.0, df = btop - t.cmm1;
-    elim(af, bf, cf, df, w.as[2], w.ds[2], w.as[1], w.ds[1]);
-}
-
-// XK(2n-1), XK(2n) -> XK1, XK2 with the underflow test of dsolver.f90:91-101.
-__device__ __forceinline__ void unmix(double xa, double xb, double &xk1, double &xk2) {
-    xk1 = xa + xb;
-    xk2 = xa - xb;
-    if (xk2 != 0.0 && fabs(xk2 / (xa + R4(1.e-20))) < R4(1.E-30)) xk2 = 0.0;
-}
-
-// 8-corner gather and interpolation (optcv.f90:279-301): returns TAUGAS.
-__device__ __forceinline__ double taugas_at(const ColSmem &s, int k, const double *__restrict__ tb) {
-    const int mt = s.mt[k] - 1, mp = s.mp[k] - 1, nh = s.nh[k] - 1;
-    const int nh1 = nh + 1 < D_NH ? nh + 1 : D_NH - 1;   // WRATIO = 0 when NH2O = 10
-    const double wr = s.wr[k];
-    auto corner = [&](int a, int b) {
-        const double *p = tb + ((size_t)(a * D_NP + b) * D_NH) * D_NGK;
-        const double c0 = __ldg(p + nh * D_NGK), c1 = __ldg(p + nh1 * D_NGK);
-        return c0 + wr * (c1 - c0);
-    };
-    const double k1 = corner(mt, mp), k2 = corner(mt, mp + 1);
-    const double k3 = corner(mt + 1, mp + 1), k4 = corner(mt + 1, mp);
-    const double ans = s.lk[4 * k] * k1 + s.lk[4 * k + 1] * k2 + s.lk[4 * k + 2] * k3 + s.lk[4 * k + 3] * k4;
-    return s.u[k] * ans;
-}
-
-// ---------------------------------------------------------------- visible
-__device__ void solve_vis(const SegDev &sg, int c, int nw, int ng, int sidx, ColSmem &s,
-                          const RtConst &K, const double *__restrict__ kv, SysLocal &w,
-                          unsigned int &nsolved) {
-    const int L = sg.L, NL = L + 1;
-    const double fz0 = K.fzerov[nw - 1];
-    const bool band_skip = ng < D_NG && fz0 >= R4(0.99);
-    const double *tb = kv + (size_t)(nw - 1) * D_NT * D_NP * D_NH * D_NGK + (ng - 1);
-    double taugsurf = 0.0;
-    auto dtauk = [&](int k) -> double {
-        if (ng < D_NG) {
-            const double tg = taugas_at(s, k, tb);
-            taugsurf += tg;
-            return tg + s.trayaer[k * D_NV + nw - 1];
-        }
-        return s.trayaer[k * D_NV + nw - 1];
-    };
-    // pass A: levels 2..LEV, TCIN prefix sums, delta-Eddington stream.
-    // a0 = W0, a1 = COSBAR, a2 = scaled DTAU, a3 = TAU (1..NL+1), a4 = TAUCUM(2l+1)
-    const double tc2 = 0.0 + dtauk(2);
-    double tc = tc2, tau = 0.0, fprev = 0.0, tcE1 = 0.0, tcLev = 0.0;
-    for (int l = 1; l <= NL; ++l) {
-        const int k = 2 * l + 1;
-        const double da = dtauk(k);
-        const double tcA = tc + da;
-        double dt, tcB;
-        if (l <= L) {
-            const double db = dtauk(k + 1);
-            tcB = tcA + db;
-            dt = da + db;
-        } else {
-            tcB = tcA;
-            dt = da;
-        }
-        const double wb = s.wnum_v[l * D_NV + nw - 1] / dt;
-        const double cb = s.cosb_v[l * D_NV + nw - 1];
-        const double f = 1.0 - wb * (cb * cb);
-        if (l == 1) {
-            tau = 0.0 * f;
-            tcE1 = tc2 * f;
-            w.a4[1] = tcE1 + (tcA - tc2) * f;
-        } else if (l < NL) {
-            w.a4[l] = tau + (tcA - tc) * fprev;
-        }
-        w.a0[l] = wb * (1.0 - cb * cb) / f;
-        w.a1[l] = cb / (1.0 + cb);
-        const double dtl = dt * f;
-        w.a2[l] = dtl;
-        w.a3[l] = tau;
-        tau = tau + dtl;
-        fprev = f;
-        tc = tcB;
-        tcLev = tcB;
-    }
-    w.a3[NL + 1] = tau;
-    const double detau = tau;
-    double *detau_o = sg.detau + (size_t)c * 119;
-    sg.cumtauv[(size_t)c * 119 + (nw - 1) + 7 * (ng - 1)] = tcLev;
-    if (band_skip) {
-        s.skip[sidx] = 2;
-        return;
-    }
-    detau_o[(nw - 1) + 7 * (ng - 1)] = detau;
-    if (ng < D_NG && taugsurf < TLIMITS) {
-        s.skip[sidx] = 1;
-        return;
-    }
-    s.skip[sidx] = 0;
-    ++nsolved;
-
-    // pass C: coefficients bottom-up, rows eliminated as generated.
-    const double u0 = sg.acosz[c], rsf = sg.als[c], f0pi = sg.sol[nw - 1];
-    const double rcp_u0 = 1.0 / u0, rcp_u02 = 1.0 / (u0 * u0);
-    const double s3 = (double)sqrtf(3.0f), s3h = (double)(sqrtf(3.0f) * 0.5f);
-    const double bsurf = rsf * u0 * sg.sol[nw - 1] * mgcm_rt_exp(-dmin(detau / u0, MAXEXP));
-    const double btop = 0.0;
-    // c0 = LAMDA, c1 = GAMA, c2 = AM, c3 = AP
-    auto coef = [&](int l, double et_top, double et_bot) {
-        Lay y;
-        const double w0 = w.a0[l], cb = w.a1[l];
-        const double g1 = s3h * (2.0 - w0 * (1.0 + cb));
-        const double g2 = (s3 * w0 * 0.5) * (1.0 - cb);
-        const double g3 = 0.5 * (1.0 - s3 * cb * u0);
-        const double lam = sqrt(g1 * g1 - g2 * g2);
-        y.gama = (g1 - lam) / g2;
-        const double g4 = 1.0 - g3;
-        double denom = lam * lam - rcp_u02;
-        if (denom == 0.0) denom = R4(1.E-10);
-        const double am = f0pi * w0 * (g4 * (g1 + rcp_u0) + g2 * g3) / denom;
-        const double ap = f0pi * w0 * (g3 * (g1 - rcp_u0) + g2 * g4) / denom;
-        w.c0[l] = lam;
-        w.c1[l] = y.gama;
-        w.c2[l] = am;
-        w.c3[l] = ap;
-        y.cpm1 = ap * et_top;
-        y.cmm1 = am * et_top;
-        y.cp = ap * et_bot;
-        y.cm = am * et_bot;
-        const double ep = mgcm_rt_exp(dmin(TAUMAX, lam * w.a2[l]));
-        const double em = 1.0 / ep;
-        y.e1 = ep + y.gama * em;
-        y.e2 = ep - y.gama * em;
-        y.e3 = y.gama * ep + em;
-        y.e4 = y.gama * ep - em;
-        return y;
-    };
-    double et_bot = mgcm_rt_exp(-dmin(w.a3[NL + 1] / u0, MAXEXP));
-    double et_top = mgcm_rt_exp(-dmin(w.a3[NL] / u0, MAXEXP));
-    Lay hi = coef(NL, et_top, et_bot);
-    bottom_row(hi, NL, bsurf, rsf, w);
-    for (int n = NL - 1; n >= 1; --n) {
-        et_bot = et_top;
-        et_top = mgcm_rt_exp(-dmin(w.a3[n] / u0, MAXEXP));
-        const Lay lo = coef(n, et_top, et_bot);
-        elim_pair(lo, hi, n, w);
-        hi = lo;
-    }
-    top_row(hi, btop, w);
-
-    // pass D: back-substitution, unmixing, midpoint fluxes.
-    double *fmp = s.fmp + (size_t)sidx * NL, *fmm = s.fmm + (size_t)sidx * NL;
-    double xprev = 0.0;
-    for (int n = 1; n <= NL; ++n) {
-        const double xa = n == 1 ? w.ds[1] : w.ds[2 * n - 1] - w.as[2 * n - 1] * xprev;
-        const double xb = w.ds[2 * n] - w.as[2 * n] * xa;
-        xprev = xb;
-        double xk1, xk2;
-        unmix(xa, xb, xk1, xk2);
-        const double lam = w.c0[n], gama = w.c1[n], am = w.c2[n], ap = w.c3[n];
-        if (n == 1) {
-            const double ep = 1.0, em = 1.0;
-            const double fup = xk1 * ep + gama * xk2 * em + ap;
-            double fdn = xk1 * ep * gama + xk2 * em + am;
-            fdn = fdn + u0 * f0pi * mgcm_rt_exp(-dmin(0.0 / u0, MAXEXP));
-            s.sc0[sidx] = fup;
-            s.sc1[sidx] = fdn;
-        }
-        if (n < NL) {
-            const double tcE = n == 1 ? tcE1 : w.a3[n];
-            const double ep = mgcm_rt_exp(dmin(TAUMAX, lam * (w.a4[n] - tcE)));
-            const double em = 1.0 / ep;
-            const double et = mgcm_rt_exp(-dmin(w.a4[n] / u0, MAXEXP));
-            const double cpmid = ap * et, cmmid = am * et;
-            fmp[n - 1] = xk1 * ep + gama * xk2 * em + cpmid;
-            double m = xk1 * ep * gama + xk2 * em + cmmid;
-            fmm[n - 1] = m + u0 * f0pi * et;
-        } else {
-            const double ep = mgcm_rt_exp(dmin(TAUMAX, lam * (w.a3[NL + 1] - w.a3[NL])));
-            const double em = 1.0 / ep;
-            const double taumid = dmin(w.a3[NL + 1], TAUMAX);
-            const double et = mgcm_rt_exp(-dmin(taumid / u0, MAXEXP));
-            const double cpmid = ap * et, cmmid = am * et;
-            fmp[n - 1] = xk1 * ep + gama * xk2 * em + cpmid;
-            const double m = xk1 * ep * gama + xk2 * em + cmmid;
-            s.sc2[sidx] = m;
-            fmm[n - 1] = m + u0 * f0pi * et;
-        }
-    }
-}
-
-// ---------------------------------------------------------------- infrared
-__device__ void solve_ir(const SegDev &sg, int c, int nw, int ng, int sidx, ColSmem &s,
-                         const RtConst &K, const double *__restrict__ ki, SysLocal &w,
-                         unsigned int &nsolved) {
-    const int L = sg.L, NL = L + 1, LEV = 2 * L + 3;
-    const double fz0 = K.fzeroi[nw - 1];
-    if (ng < D_NG && fz0 >= R4(0.99)) {
-        s.skip[sidx] = 2;
-        return;
-    }
-    const double *tb = ki + (size_t)(nw - 1) * D_NT * D_NP * D_NH * D_NGK + (ng - 1);
-    double taugsurf = 0.0;
-    auto dtauk = [&](int k) -> double {
-        const double ta = s.taer_i[k * D_NI + nw - 1], tcl = s.tcld_i[k * D_NI + nw - 1];
-        if (ng < D_NG) {
-            const double tg = taugas_at(s, k, tb);
-            taugsurf += tg;
-            return tg + ta + tcl;
-        }
-        return ta + tcl;
-    };
-    // pass A. a0 = WBARI, a1 = COSBI, a2 = DTAUI, a4 = TAUCUMI(2l+1)-TAUCUMI(2l)
-    const double tiny = R4(1.0E-9);
-    double tc = 0.0 + dtauk(2);
-    for (int l = 1; l <= NL; ++l) {
-        const int k = 2 * l + 1;
-        const double da = dtauk(k);
-        const double tcA = tc + da;
-        double dt, tcB;
-        if (k + 1 <= LEV) {
-            const double db = dtauk(k + 1);
-            tcB = tcA + db;
-            dt = da + db + 1.0e-50;
-        } else {
-            tcB = tcA;
-            dt = da + 0.0 + 1.0e-50;
-        }
-        double wb;
-        if (dt > tiny) {
-            wb = s.wnum_i[l * D_NI + nw - 1] / dt;
-        } else {
-            wb = 0.0;
-            dt = tiny;
-        }
-        w.a0[l] = wb;
-        w.a1[l] = s.cosb_i[l * D_NI + nw - 1];
-        w.a2[l] = dt;
-        if (l < NL) w.a4[l] = tcA - tc;
-        tc = tcB;
-    }
-    if (ng < D_NG && taugsurf < TLIMITI) {
-        s.skip[sidx] = 1;
-        return;
-    }
-    s.skip[sidx] = 0;
-    ++nsolved;
-    const double *plev = sg.plev + (size_t)c * LEV;
-    const double rsf = sg.albi[c];
-    const double tautop = w.a2[1] * plev[2 - 1] / (plev[4 - 1] - plev[2 - 1]);
-    const double btop = (1.0 - mgcm_rt_exp(-tautop / UBARI)) * s.pltop_i[nw - 1];
-    const double bsurf = s.bsurf_i[nw - 1];
-    // c0 = LAMDA, c1 = GAMA, c2 = B1, c3 = TERM
-    auto coef = [&](int l) {
-        Lay y;
-        const double w0 = w.a0[l], cb = w.a1[l], dt = w.a2[l];
-        const double alpha = sqrt((1.0 - w0) / (1.0 - w0 * cb));
-        const double lam = alpha * (1.0 - w0 * cb) / UBARI;
-        const double b0 = s.b0_i[l * D_NI + nw - 1];
-        const double b1 = s.pdif_i[l * D_NI + nw - 1] / dt;
-        y.gama = (1.0 - alpha) / (1.0 + alpha);
-        const double term = UBARI / (1.0 - w0 * cb);
-        y.cp = b0 + b1 * dt + b1 * term;
-        y.cm = b0 + b1 * dt - b1 * term;
-        y.cpm1 = b0 + b1 * term;
-        y.cmm1 = b0 - b1 * term;
-        const double ep = mgcm_rt_exp(dmin(lam * dt, TAUMAX));
-        const double em = 1.0 / ep;
-        y.e1 = ep + y.gama * em;
-        y.e2 = ep - y.gama * em;
-        y.e3 = y.gama * ep + em;
-        y.e4 = y.gama * ep - em;
-        w.c0[l] = lam;
-        w.c1[l] = y.gama;
-        w.c2[l] = b1;
-        w.c3[l] = term;
-        return y;
-    };
-    Lay hi = coef(NL);
-    bottom_row(hi, NL, bsurf, rsf, w);
-    for (int n = NL - 1; n >= 1; --n) {
-        const Lay lo = coef(n);
-        elim_pair(lo, hi, n, w);
-        hi = lo;
-    }
-    top_row(hi, btop, w);
-
-    double *fmp = s.fmp + (size_t)sidx * NL, *fmm = s.fmm + (size_t)sidx * NL;
-    double xprev = 0.0;
-    for (int n = 1; n <= NL; ++n) {
-        const double xa = n == 1 ? w.ds[1] : w.ds[2 * n - 1] - w.as[2 * n - 1] * xprev;
-        const double xb = w.ds[2 * n] - w.as[2 * n] * xa;
-        xprev = xb;
-        double xk1, xk2;
-        unmix(xa, xb, xk1, xk2);
-        const double lam = w.c0[n], gama = w.c1[n], b1 = w.c2[n], term = w.c3[n];
-        const double b0 = s.b0_i[n * D_NI + nw - 1];
-        const double dtk = n < NL ? w.a4[n] : w.a2[n];
-        const double ep = mgcm_rt_exp(dmin(lam * dtk, TAUMAX));
-        const double em = 1.0 / ep;
-        const double cpmid = b0 + b1 * dtk + b1 * term;
-        const double cmmid = b0 + b1 * dtk - b1 * term;
-        const double p = xk1 * ep + gama * xk2 * em + cpmid;
-        const double m = xk1 * ep * gama + xk2 * em + cmmid;
-        fmp[n - 1] = p * PI_D;
-        fmm[n - 1] = m * PI_D;
-        if (n == 1) {
-            const double ep1 = 1.0, em1 = 1.0;
-            const double cpm = b0 + b1 * term, cmm = b0 - b1 * term;
-            const double fup = xk1 * ep1 + gama * xk2 * em1 + cpm;
-            const double fdn = xk1 * ep1 * gama + xk2 * em1 + cmm;
-            s.sc0[sidx] = (fup - fdn) * PI_D;
-        }
-    }
-}
-
-// Ordered sums over (band, Gauss) of one output (code/sfluxv.f90:60-164,
-// code/sfluxi.f90:57-145).  q: 0 net, 1 up, 2 down (layer l), 3 top net, 4 DIFFV.
-__device__ double reduce_family(const ColSmem &s, const RtConst &K, bool vis, int q, int l,
-                                int NL) {
-    const int nb = vis ? D_NV : D_NI, base = vis ? 0 : NSYS_V;
-    const double *fz = vis ? K.fzerov : K.fzeroi;
-    double acc = 0.0;
-    for (int nw = 1; nw <= nb; ++nw) {
-        double fzero = fz[nw - 1];
-        const double dw = vis ? 1.0 : K.dwni[nw - 1];
-        auto val = [&](int sidx) -> double {
-            switch (q) {
-                case 0: return s.fmp[(size_t)sidx * NL + l - 1] - s.fmm[(size_t)sidx * NL + l - 1];
-                case 1: return s.fmp[(size_t)sidx * NL + l - 1];
-                case 2: return s.fmm[(size_t)sidx * NL + l - 1];
-                case 3: return vis ? s.sc0[sidx] - s.sc1[sidx] : s.sc0[sidx];
-                default: return s.sc2[sidx];
-            }
-        };
-        if (!(fzero >= R4(0.99))) {
-            for (int ng = 1; ng <= D_NG - 1; ++ng) {
-                const int sidx = base + (nw - 1) * D_NG + ng - 1;
-                if (s.skip[sidx] == 1) {
-                    fzero = fzero + (1.0 - fz[nw - 1]) * K.gweight[ng - 1];
-                    continue;
-                }
-                if (vis) acc = acc + val(sidx) * K.gweight[ng - 1] * (1.0 - fz[nw - 1]);
-                else acc = acc + val(sidx) * dw * K.gweight[ng - 1] * (1.0 - fz[nw - 1]);
-            }
-        }
-        const int s17 = base + (nw - 1) * D_NG + D_NG - 1;
-        if (vis) acc = acc + val(s17) * fzero;
-        else acc = acc + val(s17) * dw * fzero;
-    }
-    return acc;
-}
-
-}  // namespace
+using namespace fp64;
 
 __global__ void __launch_bounds__(224, 2)
 rt_fp64_kernel(const SegTable *__restrict__ st, const double *__restrict__ kv,
@@ -461,55 +54,13 @@ rt_fp64_kernel(const SegTable *__restrict__ st, const double *__restrict__ kv,
         __syncthreads();
         const int t = threadIdx.x;
         if (t < NSYS_V) {
-            if (day) solve_vis(sg, c, t / D_NG + 1, t % D_NG + 1, t, s, K, kv, w, nsolved);
+            if (day) solve_vis<0>(sg, c, t / D_NG + 1, t % D_NG + 1, t, s, K, kv, w, nsolved);
         } else if (t < NSYS) {
             const int j = t - NSYS_V;
-            solve_ir(sg, c, j / D_NG + 1, j % D_NG + 1, t, s, K, ki, w, nsolved);
+            solve_ir<0>(sg, c, j / D_NG + 1, j % D_NG + 1, t, s, K, ki, w, nsolved);
         }
         __syncthreads();
-        // ordered reductions: visible 3*NL+2 items, IR 3*NL+1 items
-        const int nv_items = 3 * NL + 2, ni_items = 3 * NL + 1;
-        for (int it = t; it < nv_items + ni_items; it += blockDim.x) {
-            const bool vis = it < nv_items;
-            const int j = vis ? it : it - nv_items;
-            int q, l = 1;
-            if (j < 3 * NL) { q = j / NL; l = j % NL + 1; }
-            else q = 3 + (j - 3 * NL);
-            double v = 0.0;
-            if (!vis || day) v = reduce_family(s, K, vis, q, l, NL);
-            const size_t o = (size_t)c * NL + l - 1;
-            if (vis) {
-                if (q == 0) { sg.fmnetv[o] = v; s.fmnet_v[l] = v; }
-                else if (q == 1) sg.fluxupv[o] = v;
-                else if (q == 2) {
-                    sg.fluxdnv[o] = v;
-                    if (l == NL) { sg.dnvflux[c] = v; sg.fluxsurf[c] = (1.0 - sg.als[c]) * v; }
-                } else if (q == 3) { sg.nfluxtopv[c] = v; s.misc[0] = v; }
-                else { sg.diffvt[c] = v; sg.dndiffv[c] = v; }
-            } else {
-                if (q == 0) { sg.fmneti[o] = v; s.fmnet_i[l] = v; }
-                else if (q == 1) sg.fluxupi[o] = v;
-                else if (q == 2) { sg.fluxdni[o] = v; if (l == NL) sg.dnirflux[c] = v; }
-                else { sg.nfluxtopi[c] = v; s.misc[1] = v; }
-            }
-        }
-        __syncthreads();
-        // divergences and heating rates
-        const double *plev = sg.plev + (size_t)c * LEV;
-        for (int l = 1 + t; l <= NL; l += blockDim.x) {
-            const double sun = day ? (l == 1 ? s.fmnet_v[1] - s.misc[0] : s.fmnet_v[l] - s.fmnet_v[l - 1]) : 0.0;
-            const double irt = l == 1 ? s.fmnet_i[1] - s.misc[1] : s.fmnet_i[l] - s.fmnet_i[l - 1];
-            const int k = 2 * l;
-            const double ptrop = sg.ptrop, p = sg.pcol[c];
-            const double ym = k == 2 ? ptrop * 100.0 / 3.72 : (plev[k + 1 - 1] - plev[k - 1 - 1]) * 100.0 / 3.72;
-            const double om = pow(plev[k - 1] / plev[LEV - 1], 0.25684);
-            const double pnlte = sg.sigma[k - 1] * (p - ptrop) + ptrop;
-            const double sunlte = sun * 2.2e4 * pnlte / (1.0 + 2.2e4 * pnlte);
-            const size_t o = (size_t)c * NL + l - 1;
-            sg.suntot[o] = sun;
-            sg.irtotal[o] = irt;
-            sg.qrad[o] = (sunlte + irt) / (735.94 * ym * om);
-        }
+        reduce_and_heat(sg, c, s, K, day);
         __syncthreads();
     }
     if (nsys) {
@@ -517,6 +68,122 @@ rt_fp64_kernel(const SegTable *__restrict__ st, const double *__restrict__ kv,
         unsigned int v = nsolved;
         for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
         if ((threadIdx.x & 31) == 0 && v) atomicAdd(nsys, (unsigned long long)v);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Three-kernel pipeline over a chunk of columns [col_begin, col_end).  Each
+// column owns a block of global memory laid out like the fused kernel's shared
+// memory (ColSmem, stride bytes): the stage data, the TLIMIT flags and the
+// per-system midpoint fluxes.  Solved systems are listed per family so the
+// solver keeps every thread busy (night columns and TLIMIT skips drop out).
+
+// K1: stage the column and screen every system (optics sums, TLIMIT test,
+// DETAU, CUMTAUV); append kept systems to the family lists.
+__global__ void __launch_bounds__(224)
+rt_fp64_screen(const SegTable *__restrict__ st, int col_begin, int col_end, int max_nl,
+               unsigned char *__restrict__ blocks, size_t stride, const double *__restrict__ kv,
+               const double *__restrict__ ki, const double *__restrict__ planck, const RtConst K,
+               int *__restrict__ list_v, int *__restrict__ list_i, unsigned int *counts,
+               uint32_t *status, unsigned long long *nsys) {
+    __shared__ int warp_v[8], warp_i[8], base_v, base_i;
+    SysLocal w;
+    unsigned int nsolved = 0;
+    const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
+    for (int g = col_begin + blockIdx.x; g < col_end; g += gridDim.x) {
+        const int si = find_seg(st, g);
+        const SegDev &sg = st->seg[si];
+        const int c = g - sg.col0;
+        ColSmem s = carve_smem(blocks + (size_t)(g - col_begin) * stride, max_nl);
+        const bool day = sg.acosz[c] >= R4(1.0e-5);
+        stage_column(sg, c, K, planck, s, status);
+        __syncthreads();
+        bool act_v = false, act_i = false;
+        if (t < NSYS_V) {
+            if (day) {
+                solve_vis<1>(sg, c, t / D_NG + 1, t % D_NG + 1, t, s, K, kv, w, nsolved);
+                act_v = s.skip[t] == 0;
+            }
+        } else if (t < NSYS) {
+            const int j = t - NSYS_V;
+            solve_ir<1>(sg, c, j / D_NG + 1, j % D_NG + 1, t, s, K, ki, w, nsolved);
+            act_i = s.skip[t] == 0;
+        }
+        const unsigned bv = __ballot_sync(0xffffffffu, act_v), bi = __ballot_sync(0xffffffffu, act_i);
+        if (lane == 0) {
+            warp_v[wid] = __popc(bv);
+            warp_i[wid] = __popc(bi);
+        }
+        __syncthreads();
+        if (t == 0) {
+            int nv = 0, ni = 0;
+            for (int q = 0; q < (int)(blockDim.x >> 5); ++q) {
+                const int a = warp_v[q], b = warp_i[q];
+                warp_v[q] = nv;
+                warp_i[q] = ni;
+                nv += a;
+                ni += b;
+            }
+            base_v = nv ? (int)atomicAdd(&counts[0], (unsigned)nv) : 0;
+            base_i = ni ? (int)atomicAdd(&counts[1], (unsigned)ni) : 0;
+        }
+        __syncthreads();
+        const unsigned below = (1u << lane) - 1u;
+        if (act_v) list_v[base_v + warp_v[wid] + __popc(bv & below)] = (g << 8) | t;
+        if (act_i) list_i[base_i + warp_i[wid] + __popc(bi & below)] = (g << 8) | t;
+        __syncthreads();
+    }
+    if (nsys) {
+        unsigned int v = nsolved;
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0 && v) atomicAdd(nsys, (unsigned long long)v);
+    }
+}
+
+// K2: solve the listed systems of one family, one thread per system.
+template <bool VIS>
+__global__ void __launch_bounds__(128)
+rt_fp64_solve(const SegTable *__restrict__ st, int col_begin, int max_nl,
+              unsigned char *__restrict__ blocks, size_t stride, const double *__restrict__ ktab,
+              const RtConst K, const int *__restrict__ list, const unsigned int *count) {
+    SysLocal w;
+    unsigned int dummy = 0;
+    const unsigned int n = VIS ? count[0] : count[1];
+    for (unsigned int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int e = list[i];
+        const int g = e >> 8, sidx = e & 255;
+        const int si = find_seg(st, g);
+        const SegDev &sg = st->seg[si];
+        const int c = g - sg.col0;
+        ColSmem s = carve_smem(blocks + (size_t)(g - col_begin) * stride, max_nl);
+        if (VIS) {
+            solve_vis<2>(sg, c, sidx / D_NG + 1, sidx % D_NG + 1, sidx, s, K, ktab, w, dummy);
+        } else {
+            const int j = sidx - NSYS_V;
+            solve_ir<2>(sg, c, j / D_NG + 1, j % D_NG + 1, sidx, s, K, ktab, w, dummy);
+        }
+    }
+}
+
+template __global__ void rt_fp64_solve<true>(const SegTable *__restrict__, int, int, unsigned char *__restrict__,
+                                             size_t, const double *__restrict__, const RtConst,
+                                             const int *__restrict__, const unsigned int *);
+template __global__ void rt_fp64_solve<false>(const SegTable *__restrict__, int, int, unsigned char *__restrict__,
+                                              size_t, const double *__restrict__, const RtConst,
+                                              const int *__restrict__, const unsigned int *);
+
+// K3: ordered sums and heating per column.
+__global__ void __launch_bounds__(160)
+rt_fp64_reduce(const SegTable *__restrict__ st, int col_begin, int col_end, int max_nl,
+               unsigned char *__restrict__ blocks, size_t stride, const RtConst K) {
+    for (int g = col_begin + blockIdx.x; g < col_end; g += gridDim.x) {
+        const int si = find_seg(st, g);
+        const SegDev &sg = st->seg[si];
+        const int c = g - sg.col0;
+        ColSmem s = carve_smem(blocks + (size_t)(g - col_begin) * stride, max_nl);
+        const bool day = sg.acosz[c] >= R4(1.0e-5);
+        reduce_and_heat(sg, c, s, K, day);
+        __syncthreads();
     }
 }
 
