@@ -8,6 +8,7 @@
 #include <cmath>
 #include <condition_variable>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <map>
@@ -36,10 +37,14 @@ template <bool VIS>
 __global__ void rt_fp64_solve(const SegTable *__restrict__ st, int col_begin, int max_nl,
                               unsigned char *__restrict__ blocks, size_t stride,
                               const double *__restrict__ ktab, const RtConst K,
-                              const int *__restrict__ list, const unsigned int *count);
+                              const int *__restrict__ list, const unsigned int *count,
+                              double *__restrict__ fl, double *__restrict__ sc);
 __global__ void rt_fp64_reduce(const SegTable *__restrict__ st, int col_begin, int col_end,
                                int max_nl, unsigned char *__restrict__ blocks, size_t stride,
-                               const RtConst K);
+                               const RtConst K, const double *__restrict__ fl_v,
+                               const double *__restrict__ sc_v, const double *__restrict__ fl_i,
+                               const double *__restrict__ sc_i, uint32_t *status, int in_smem);
+size_t reduce_smem_bytes(int max_nl, int rows);
 __global__ void rt_dsolflux_kernel(int ncol, const double *__restrict__ sol,
                                    const double *__restrict__ acosz,
                                    const double *__restrict__ detau,
@@ -135,7 +140,7 @@ struct mgcm_rt_handle {
     Arena stage;                  // host-pointer staging
     Arena red;                    // flux staging for L too large for shared memory
     Arena pipe;                   // pipeline: per-column blocks, system lists, counters
-    int occ_screen = 0, occ_solve = 0, occ_reduce = 0;
+    int occ_screen = 0, occ_solve = 0, occ_reduce = 0, occ_nl = 0;
     std::mutex mu;
     mgcm_rt_stats stats{};
     size_t budget = 0;
@@ -297,11 +302,15 @@ int fp64_blocks_per_sm(int max_nl) {
 
 // Three-kernel FP64 pipeline over chunks of columns (rt_fp64.cu).
 int launch_pipeline(mgcm_rt_handle *h, int total, int max_nl, int &nk) {
-    const size_t stride = (col_smem_bytes(max_nl, true) + 255) / 256 * 256;
-    const size_t per_col = stride + 2 * NSYS * sizeof(int);
+    auto al = [](size_t b) { return (b + 255) / 256 * 256; };
+    const size_t stride = al(col_smem_bytes(max_nl, false));
+    const size_t row = (size_t)2 * max_nl * sizeof(double);
+    const size_t per_col = stride + NSYS * (sizeof(int) + row + 4 * sizeof(double));
     const size_t cap = std::min<size_t>(h->budget / 2, (size_t)8 << 30);
-    int chunk = (int)std::min<size_t>((size_t)total, std::max<size_t>(cap / per_col, 1));
-    const size_t need = (size_t)chunk * per_col + 256;
+    const int chunk = (int)std::min<size_t>((size_t)total, std::max<size_t>(cap / per_col, 1));
+    const size_t n_v = (size_t)chunk * NSYS_V, n_i = (size_t)chunk * NSYS_I;
+    const size_t need = al((size_t)chunk * stride) + al(n_v * 4) + al(n_i * 4) + al(n_v * row) +
+                        al(n_i * row) + al(n_v * 32) + al(n_i * 32) + 256;
     if (h->pipe.bytes < need) {
         if (h->pipe.ptr) {
             CK(cudaStreamSynchronize(h->stream));
@@ -312,17 +321,33 @@ int launch_pipeline(mgcm_rt_handle *h, int total, int max_nl, int &nk) {
         if (cudaMalloc(&h->pipe.ptr, need) != cudaSuccess) return MGCM_RT_ENOMEM;
         h->pipe.bytes = need;
     }
-    unsigned char *blocks = static_cast<unsigned char *>(h->pipe.ptr);
-    int *list_v = reinterpret_cast<int *>(blocks + (size_t)chunk * stride);
-    int *list_i = list_v + (size_t)chunk * NSYS_V;
-    unsigned int *counts = reinterpret_cast<unsigned int *>(list_i + (size_t)chunk * NSYS_I);
-    if (!h->occ_screen) {
+    unsigned char *p = static_cast<unsigned char *>(h->pipe.ptr);
+    auto take = [&](size_t b) { unsigned char *r = p; p += al(b); return r; };
+    unsigned char *blocks = take((size_t)chunk * stride);
+    int *list_v = reinterpret_cast<int *>(take(n_v * 4));
+    int *list_i = reinterpret_cast<int *>(take(n_i * 4));
+    double *fl_v = reinterpret_cast<double *>(take(n_v * row));
+    double *fl_i = reinterpret_cast<double *>(take(n_i * row));
+    double *sc_v = reinterpret_cast<double *>(take(n_v * 32));
+    double *sc_i = reinterpret_cast<double *>(take(n_i * 32));
+    unsigned int *counts = reinterpret_cast<unsigned int *>(take(256));
+    // reduce pool: room for a typical column's kept systems in ~48 KB (4 CTAs
+    // per SM); columns with more kept systems sum from global memory
+    int pool_rows = (int)std::min<size_t>(NSYS, (48 * 1024) / (16 * (size_t)max_nl + 32));
+    if (pool_rows < 24) pool_rows = 0;
+    const size_t rsm = reduce_smem_bytes(max_nl, pool_rows);
+    const bool rin = pool_rows > 0;
+    if (h->occ_nl != max_nl) {
+        h->occ_nl = max_nl;
         int a = 1, b = 1, c = 1;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, rt_fp64_screen, BLOCK, 0);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, rt_fp64_solve<false>, 128, 0);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, rt_fp64_reduce, 160, 0);
+        cudaFuncSetAttribute(rt_fp64_reduce, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             rin ? (int)rsm : 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, rt_fp64_reduce, 160, rin ? rsm : 0);
         h->occ_screen = std::max(a, 1);
         h->occ_solve = std::max(b, 1);
+        if (const char *e = std::getenv("MGCM_RT_SOLVE_CTAS_PER_SM")) h->occ_solve = std::max(1, std::atoi(e));
         h->occ_reduce = std::max(c, 1);
     }
     for (int c0 = 0; c0 < total; c0 += chunk) {
@@ -334,11 +359,13 @@ int launch_pipeline(mgcm_rt_handle *h, int total, int max_nl, int &nk) {
                                                      list_i, counts, h->d_status, h->d_nsys);
         const int g2 = h->num_sms * h->occ_solve;
         rt_fp64_solve<true><<<g2, 128, 0, h->stream>>>(h->d_segs, c0, max_nl, blocks, stride,
-                                                        h->d_kv, h->K, list_v, counts);
+                                                        h->d_kv, h->K, list_v, counts, fl_v, sc_v);
         rt_fp64_solve<false><<<g2, 128, 0, h->stream>>>(h->d_segs, c0, max_nl, blocks, stride,
-                                                         h->d_ki, h->K, list_i, counts);
+                                                         h->d_ki, h->K, list_i, counts, fl_i, sc_i);
         const int g3 = std::min(c1 - c0, h->num_sms * h->occ_reduce);
-        rt_fp64_reduce<<<g3, 160, 0, h->stream>>>(h->d_segs, c0, c1, max_nl, blocks, stride, h->K);
+        rt_fp64_reduce<<<g3, 160, rin ? rsm : 0, h->stream>>>(h->d_segs, c0, c1, max_nl, blocks,
+                                                               stride, h->K, fl_v, sc_v, fl_i, sc_i,
+                                                               h->d_status, pool_rows);
         nk += 4;
         CK(cudaGetLastError());
     }
@@ -389,6 +416,7 @@ int launch_all(mgcm_rt_handle *h, int total, int max_nl, bool validate) {
 }
 
 int status_to_code(uint32_t st) {
+    if (st & 16u) return MGCM_RT_ECUDA;   // a bounded device wait ran out
     if (st & ST_NONFINITE) return MGCM_RT_ENONFINITE;
     if (st & (ST_TEMP | ST_PLANCK_RANGE)) return MGCM_RT_ETEMP;
     if (st & ST_BADL) return MGCM_RT_ELAYERS;

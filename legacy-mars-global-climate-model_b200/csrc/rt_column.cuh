@@ -35,6 +35,7 @@ struct ColSmem {
     double *fmp, *fmm;                  // [sys][l]
     double *sc0, *sc1, *sc2;            // [sys] FLUXUP, FLUXDN, DIFFV (vis) / FTOPUP (IR)
     unsigned char *skip;                // [sys] 0 = solved, 1 = TLIMIT skip, 2 = no work
+    int *meta;                          // [4] list base/count of kept systems: vis, IR
     double *fmnet_v, *fmnet_i;          // [l] reduced net fluxes for the divergences
     double *misc;                       // [4] NFLUXTOPV, NFLUXTOPI
     int day;
@@ -63,7 +64,8 @@ __host__ __device__ inline size_t col_smem_bytes(int nl, bool red_in_smem = true
     return b;
 }
 
-__device__ inline ColSmem carve_smem(unsigned char *base, int nl, double *red_global = nullptr) {
+__device__ inline ColSmem carve_smem(unsigned char *base, int nl, double *red_global = nullptr,
+                                     bool with_red = true) {
     ColSmem s;
     const int lev1 = 2 * nl + 3;
     double *d = reinterpret_cast<double *>(base);
@@ -86,7 +88,9 @@ __device__ inline ColSmem carve_smem(unsigned char *base, int nl, double *red_gl
     s.pdif_i = take((nl + 1) * D_NI);
     s.bsurf_i = take(D_NI);
     s.pltop_i = take(D_NI);
-    if (red_global) {
+    if (!with_red) {
+        s.fmp = s.fmm = nullptr;
+    } else if (red_global) {
         s.fmp = red_global;
         s.fmm = red_global + (size_t)NSYS * nl;
     } else {
@@ -104,6 +108,7 @@ __device__ inline ColSmem carve_smem(unsigned char *base, int nl, double *red_gl
     s.mp = ip + (lev1 + 1);
     s.nh = ip + 2 * (lev1 + 1);
     s.skip = reinterpret_cast<unsigned char *>(ip + 3 * (lev1 + 1));
+    s.meta = reinterpret_cast<int *>(((reinterpret_cast<uintptr_t>(s.skip + NSYS) + 15) / 16) * 16);
     s.day = 0;
     return s;
 }

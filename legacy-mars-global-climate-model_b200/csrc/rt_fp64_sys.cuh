@@ -95,7 +95,8 @@ __device__ __forceinline__ double taugas_at(const ColSmem &s, int k, const doubl
 template <int MODE>
 __device__ void solve_vis(const SegDev &sg, int c, int nw, int ng, int sidx, ColSmem &s,
                           const RtConst &K, const double *__restrict__ kv, SysLocal &w,
-                          unsigned int &nsolved) {
+                          unsigned int &nsolved, double *fmp, double *fmm, double *sc0,
+                          double *sc1, double *sc2) {
     const int L = sg.L, NL = L + 1;
     const double fz0 = K.fzerov[nw - 1];
     const bool band_skip = ng < D_NG && fz0 >= R4(0.99);
@@ -219,7 +220,6 @@ __device__ void solve_vis(const SegDev &sg, int c, int nw, int ng, int sidx, Col
     top_row(hi, btop, w);
 
     // pass D: back-substitution, unmixing, midpoint fluxes.
-    double *fmp = s.fmp + (size_t)sidx * NL, *fmm = s.fmm + (size_t)sidx * NL;
     double xprev = 0.0;
     for (int n = 1; n <= NL; ++n) {
         const double xa = n == 1 ? w.ds[1] : w.ds[2 * n - 1] - w.as[2 * n - 1] * xprev;
@@ -233,8 +233,8 @@ __device__ void solve_vis(const SegDev &sg, int c, int nw, int ng, int sidx, Col
             const double fup = xk1 * ep + gama * xk2 * em + ap;
             double fdn = xk1 * ep * gama + xk2 * em + am;
             fdn = fdn + u0 * f0pi * mgcm_rt_exp(-dmin(0.0 / u0, MAXEXP));
-            s.sc0[sidx] = fup;
-            s.sc1[sidx] = fdn;
+            *sc0 = fup;
+            *sc1 = fdn;
         }
         if (n < NL) {
             const double tcE = n == 1 ? tcE1 : w.a3[n];
@@ -253,7 +253,7 @@ __device__ void solve_vis(const SegDev &sg, int c, int nw, int ng, int sidx, Col
             const double cpmid = ap * et, cmmid = am * et;
             fmp[n - 1] = xk1 * ep + gama * xk2 * em + cpmid;
             const double m = xk1 * ep * gama + xk2 * em + cmmid;
-            s.sc2[sidx] = m;
+            *sc2 = m;
             fmm[n - 1] = m + u0 * f0pi * et;
         }
     }
@@ -263,7 +263,7 @@ __device__ void solve_vis(const SegDev &sg, int c, int nw, int ng, int sidx, Col
 template <int MODE>
 __device__ void solve_ir(const SegDev &sg, int c, int nw, int ng, int sidx, ColSmem &s,
                          const RtConst &K, const double *__restrict__ ki, SysLocal &w,
-                         unsigned int &nsolved) {
+                         unsigned int &nsolved, double *fmp, double *fmm, double *sc0) {
     const int L = sg.L, NL = L + 1, LEV = 2 * L + 3;
     const double fz0 = K.fzeroi[nw - 1];
     if (ng < D_NG && fz0 >= R4(0.99)) {
@@ -306,7 +306,6 @@ __device__ void solve_ir(const SegDev &sg, int c, int nw, int ng, int sidx, ColS
         }
         if (MODE != 1) {
             w.a0[l] = wb;
-            w.a1[l] = s.cosb_i[l * D_NI + nw - 1];
             w.a2[l] = dt;
             if (l < NL) w.a4[l] = tcA - tc;
         }
@@ -329,7 +328,7 @@ __device__ void solve_ir(const SegDev &sg, int c, int nw, int ng, int sidx, ColS
     // c0 = LAMDA, c1 = GAMA, c2 = B1, c3 = TERM
     auto coef = [&](int l) {
         Lay y;
-        const double w0 = w.a0[l], cb = w.a1[l], dt = w.a2[l];
+        const double w0 = w.a0[l], cb = s.cosb_i[l * D_NI + nw - 1], dt = w.a2[l];
         const double alpha = sqrt((1.0 - w0) / (1.0 - w0 * cb));
         const double lam = alpha * (1.0 - w0 * cb) / UBARI;
         const double b0 = s.b0_i[l * D_NI + nw - 1];
@@ -361,7 +360,6 @@ __device__ void solve_ir(const SegDev &sg, int c, int nw, int ng, int sidx, ColS
     }
     top_row(hi, btop, w);
 
-    double *fmp = s.fmp + (size_t)sidx * NL, *fmm = s.fmm + (size_t)sidx * NL;
     double xprev = 0.0;
     for (int n = 1; n <= NL; ++n) {
         const double xa = n == 1 ? w.ds[1] : w.ds[2 * n - 1] - w.as[2 * n - 1] * xprev;
@@ -385,7 +383,7 @@ __device__ void solve_ir(const SegDev &sg, int c, int nw, int ng, int sidx, ColS
             const double cpm = b0 + b1 * term, cmm = b0 - b1 * term;
             const double fup = xk1 * ep1 + gama * xk2 * em1 + cpm;
             const double fdn = xk1 * ep1 * gama + xk2 * em1 + cmm;
-            s.sc0[sidx] = (fup - fdn) * PI_D;
+            *sc0 = (fup - fdn) * PI_D;
         }
     }
 }
@@ -428,9 +426,79 @@ __device__ double reduce_family(const ColSmem &s, const RtConst &K, bool vis, in
 }
 
 
+// Per-row multipliers of the compact layout for one family of a column: the
+// kept systems in ascending order get m1,m2,m3 so that the reference's term
+// is ((val*m1)*m2)*m3 -- visible (val*GWEIGHT)*(1-FZEROV) or val*FZERO for
+// Gauss point 17; IR ((val*DWNI)*GWEIGHT)*(1-FZEROI) or (val*DWNI)*FZERO
+// (code/sfluxv.f90:102-162, code/sfluxi.f90:95-143).  Unused factors are
+// exactly 1.0, which leaves the product bit-identical.  Returns the rows.
+__device__ int family_multipliers(const unsigned char *skip, const RtConst &K, bool vis,
+                                  double *m1, double *m2, double *m3) {
+    const int nb = vis ? D_NV : D_NI, base = vis ? 0 : NSYS_V;
+    const double *fz = vis ? K.fzerov : K.fzeroi;
+    int pos = 0;
+    for (int nw = 1; nw <= nb; ++nw) {
+        double fzero = fz[nw - 1];
+        const double dw = vis ? 1.0 : K.dwni[nw - 1];
+        if (!(fzero >= R4(0.99))) {
+            for (int ng = 1; ng <= D_NG - 1; ++ng) {
+                const int sidx = base + (nw - 1) * D_NG + ng - 1;
+                if (skip[sidx] != 0) {
+                    fzero = fzero + (1.0 - fz[nw - 1]) * K.gweight[ng - 1];
+                    continue;
+                }
+                if (vis) {
+                    m1[pos] = K.gweight[ng - 1];
+                    m2[pos] = 1.0 - fz[nw - 1];
+                    m3[pos] = 1.0;
+                } else {
+                    m1[pos] = dw;
+                    m2[pos] = K.gweight[ng - 1];
+                    m3[pos] = 1.0 - fz[nw - 1];
+                }
+                ++pos;
+            }
+        }
+        if (vis) {
+            m1[pos] = fzero;
+            m2[pos] = 1.0;
+        } else {
+            m1[pos] = dw;
+            m2[pos] = fzero;
+        }
+        m3[pos] = 1.0;
+        ++pos;
+    }
+    return pos;
+}
+
+// Ordered sum of one output over the family's kept rows (q: 0 net, 1 up,
+// 2 down at layer l; 3 top net; 4 DIFFV).
+__device__ __forceinline__ double reduce_rows(const double *fl, const double *sc, int mnl, int rows,
+                                              const double *m1, const double *m2,
+                                              const double *m3, bool vis, int q, int l) {
+    double acc = 0.0;
+    const size_t stride = (size_t)2 * mnl;
+    if (q < 3) {
+        const double *p = fl + (l - 1);
+        for (int r = 0; r < rows; ++r, p += stride) {
+            const double v = q == 0 ? p[0] - p[mnl] : (q == 1 ? p[0] : p[mnl]);
+            acc = acc + v * m1[r] * m2[r] * m3[r];
+        }
+    } else {
+        for (int r = 0; r < rows; ++r) {
+            const double v = q == 3 ? (vis ? sc[r * 4] - sc[r * 4 + 1] : sc[r * 4]) : sc[r * 4 + 2];
+            acc = acc + v * m1[r] * m2[r] * m3[r];
+        }
+    }
+    return acc;
+}
+
 // Ordered band/Gauss sums of one column, then SUNTOT, IRTOTAL and QRAD
 // (code/comp3.f:677-681,735-747,765-771).  Called by all threads of a CTA.
-__device__ void reduce_and_heat(const SegDev &sg, int c, ColSmem &s, const RtConst &K, bool day) {
+template <class Red>
+__device__ void reduce_and_heat(const SegDev &sg, int c, Red red, double *fmnet_v, double *fmnet_i,
+                                double *misc, bool day) {
     const int L = sg.L, NL = L + 1, LEV = 2 * L + 3;
     const int t = threadIdx.x;
     // ordered reductions: visible 3*NL+2 items, IR 3*NL+1 items
@@ -442,29 +510,29 @@ __device__ void reduce_and_heat(const SegDev &sg, int c, ColSmem &s, const RtCon
         if (j < 3 * NL) { q = j / NL; l = j % NL + 1; }
         else q = 3 + (j - 3 * NL);
         double v = 0.0;
-        if (!vis || day) v = reduce_family(s, K, vis, q, l, NL);
+        if (!vis || day) v = red(vis, q, l);
         const size_t o = (size_t)c * NL + l - 1;
         if (vis) {
-            if (q == 0) { sg.fmnetv[o] = v; s.fmnet_v[l] = v; }
+            if (q == 0) { sg.fmnetv[o] = v; fmnet_v[l] = v; }
             else if (q == 1) sg.fluxupv[o] = v;
             else if (q == 2) {
                 sg.fluxdnv[o] = v;
                 if (l == NL) { sg.dnvflux[c] = v; sg.fluxsurf[c] = (1.0 - sg.als[c]) * v; }
-            } else if (q == 3) { sg.nfluxtopv[c] = v; s.misc[0] = v; }
+            } else if (q == 3) { sg.nfluxtopv[c] = v; misc[0] = v; }
             else { sg.diffvt[c] = v; sg.dndiffv[c] = v; }
         } else {
-            if (q == 0) { sg.fmneti[o] = v; s.fmnet_i[l] = v; }
+            if (q == 0) { sg.fmneti[o] = v; fmnet_i[l] = v; }
             else if (q == 1) sg.fluxupi[o] = v;
             else if (q == 2) { sg.fluxdni[o] = v; if (l == NL) sg.dnirflux[c] = v; }
-            else { sg.nfluxtopi[c] = v; s.misc[1] = v; }
+            else { sg.nfluxtopi[c] = v; misc[1] = v; }
         }
     }
     __syncthreads();
     // divergences and heating rates
     const double *plev = sg.plev + (size_t)c * LEV;
     for (int l = 1 + t; l <= NL; l += blockDim.x) {
-        const double sun = day ? (l == 1 ? s.fmnet_v[1] - s.misc[0] : s.fmnet_v[l] - s.fmnet_v[l - 1]) : 0.0;
-        const double irt = l == 1 ? s.fmnet_i[1] - s.misc[1] : s.fmnet_i[l] - s.fmnet_i[l - 1];
+        const double sun = day ? (l == 1 ? fmnet_v[1] - misc[0] : fmnet_v[l] - fmnet_v[l - 1]) : 0.0;
+        const double irt = l == 1 ? fmnet_i[1] - misc[1] : fmnet_i[l] - fmnet_i[l - 1];
         const int k = 2 * l;
         const double ptrop = sg.ptrop, p = sg.pcol[c];
         const double ym = k == 2 ? ptrop * 100.0 / 3.72 : (plev[k + 1 - 1] - plev[k - 1 - 1]) * 100.0 / 3.72;
