@@ -1,13 +1,20 @@
-// C ABI of the B200 radiation path (include/mgcm_rt.h).
+// C ABI of the B200 radiation path (include/mgcm_rt.h): handles, slots,
+// the synchronous and asynchronous batch calls and the serving queue.
+//
+// A slot is one CUDA stream with its own staging (host-pointer batches),
+// pipeline scratch, segment descriptor and status words.  A job is up to one
+// slot's worth of columns from one batch.  Synchronous calls with host
+// buffers run their jobs on two slots alternately so copies of one job
+// overlap the kernels of the other; served requests are split into jobs that
+// a worker thread admits onto free slots as memory and slots free up, so
+// work from different requests overlaps on the device.
 #include <cuda_runtime.h>
 
 #include <algorithm>
-#include <cstddef>
-#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <condition_variable>
-#include <cstdio>
+#include <cstddef>
 #include <cstdlib>
 #include <cstring>
 #include <deque>
@@ -27,23 +34,32 @@ __global__ void rt_fp64_kernel(const SegTable *__restrict__ st, const double *__
                                const double *__restrict__ ki, const double *__restrict__ planck,
                                const RtConst K, int max_nl, uint32_t *status,
                                unsigned long long *nsys, double *red_scratch);
+template <bool F32>
 __global__ void rt_fp64_screen(const SegTable *__restrict__ st, int col_begin, int col_end, int max_nl,
                                unsigned char *__restrict__ blocks, size_t stride,
                                const double *__restrict__ kv, const double *__restrict__ ki,
                                const double *__restrict__ planck, const RtConst K,
                                int *__restrict__ list_v, int *__restrict__ list_i,
-                               unsigned int *counts, uint32_t *status, unsigned long long *nsys);
+                               unsigned int *counts, uint32_t *status, unsigned long long *nsys,
+                               const float *__restrict__ kvf, const float *__restrict__ kif);
 template <bool VIS>
 __global__ void rt_fp64_solve(const SegTable *__restrict__ st, int col_begin, int max_nl,
                               unsigned char *__restrict__ blocks, size_t stride,
                               const double *__restrict__ ktab, const RtConst K,
                               const int *__restrict__ list, const unsigned int *count,
                               double *__restrict__ fl, double *__restrict__ sc);
+template <bool VIS>
+__global__ void rt_mixed_solve(const SegTable *__restrict__ st, int col_begin, int max_nl,
+                               unsigned char *__restrict__ blocks, size_t stride,
+                               const float *__restrict__ ktabf, const double *__restrict__ ktab,
+                               const RtConst K, const int *__restrict__ list,
+                               const unsigned int *count, double *__restrict__ fl,
+                               double *__restrict__ sc);
 __global__ void rt_fp64_reduce(const SegTable *__restrict__ st, int col_begin, int col_end,
                                int max_nl, unsigned char *__restrict__ blocks, size_t stride,
                                const RtConst K, const double *__restrict__ fl_v,
                                const double *__restrict__ sc_v, const double *__restrict__ fl_i,
-                               const double *__restrict__ sc_i, uint32_t *status, int in_smem);
+                               const double *__restrict__ sc_i, uint32_t *status, int pool_rows);
 size_t reduce_smem_bytes(int max_nl, int rows);
 __global__ void rt_dsolflux_kernel(int ncol, const double *__restrict__ sol,
                                    const double *__restrict__ acosz,
@@ -57,6 +73,9 @@ using namespace mgcm;
 namespace {
 
 constexpr int BLOCK = 224;
+constexpr int SYNC_JOB_COLS = 16384;    // columns per job of a synchronous host-buffer call
+constexpr int SERVE_JOB_COLS = 32768;   // columns per job of a served request
+constexpr int SERVE_SLOTS = 4;          // serving slots at most
 
 // ---------------------------------------------------------------- validation
 __global__ void validate_kernel(const SegTable *__restrict__ st, uint32_t *status) {
@@ -116,7 +135,32 @@ struct Arena {
     size_t bytes = 0;
 };
 
-struct Request;
+struct Request {
+    std::vector<mgcm_rt_batch_in> in;
+    std::vector<mgcm_rt_batch_out> out;
+    int status = 0;
+    int jobs_left = 0;
+    bool done = false;
+    std::chrono::steady_clock::time_point t_submit, t_done;
+};
+
+struct Job {
+    std::shared_ptr<Request> req;
+    int seg = 0, c0 = 0, c1 = 0;   // columns [c0, c1) of batch `seg`
+};
+
+struct Slot {
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, done = nullptr;
+    SegTable *h_segs = nullptr, *d_segs = nullptr;
+    uint32_t *d_status = nullptr, *h_status = nullptr;
+    unsigned long long *d_nsys = nullptr, *h_nsys = nullptr;
+    Arena stage, pipe, red;
+    int occ_nl = 0, occ_screen = 1, occ_solve = 1, occ_reduce = 1;
+    bool busy = false;
+    Job job;
+    int kernels = 0;
+};
 
 }  // namespace
 
@@ -124,47 +168,35 @@ struct mgcm_rt_handle {
     mgcm_rt_config cfg{};
     int device = 0;
     int num_sms = 0;
-    cudaStream_t stream = nullptr;
-    cudaStream_t own_stream = nullptr;
-    bool pending = false;
-    long long pending_cols = 0;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     HostTables host;
     RtConst K{};
     double *d_kv = nullptr, *d_ki = nullptr, *d_planck = nullptr;
     float *d_kvf = nullptr, *d_kif = nullptr;
-    uint32_t *d_status = nullptr;
-    unsigned long long *d_nsys = nullptr;
-    SegTable *d_segs = nullptr;
-    SegTable *h_segs = nullptr;   // pinned
-    Arena stage;                  // host-pointer staging
-    Arena red;                    // flux staging for L too large for shared memory
-    Arena pipe;                   // pipeline: per-column blocks, system lists, counters
-    int occ_screen = 0, occ_solve = 0, occ_reduce = 0, occ_nl = 0;
-    std::mutex mu;
+    std::mutex mu;                                  // serialises the synchronous API
+    std::vector<std::unique_ptr<Slot>> slots;       // [0], [1]: synchronous calls
+    cudaStream_t user_stream = nullptr;             // mgcm_rt_set_stream
+    cudaEvent_t fork = nullptr, join0 = nullptr, join1 = nullptr;
+    bool pending = false;
+    long long pending_cols = 0;
     mgcm_rt_stats stats{};
-    size_t budget = 0;
+    size_t budget = 0, used = 0;
+    std::mutex mem_mu;
     // serving
     std::mutex qmu;
-    std::condition_variable qcv;
+    std::condition_variable qcv, dcv;
+    std::deque<Job> jobs;
     std::map<long long, std::shared_ptr<Request>> reqs;
     long long next_ticket = 1;
+    std::vector<std::unique_ptr<Slot>> sslots;
+    std::thread worker;
+    bool stop = false;
 };
 
 namespace {
 
-struct Request {
-    mgcm_rt_batch_in in;
-    mgcm_rt_batch_out out;
-    int status = 1;   // 1 pending, 0 done, <0 error
-    bool done = false;
-};
-
-int cuda_err(cudaError_t e) { return e == cudaSuccess ? MGCM_RT_OK : MGCM_RT_ECUDA; }
-
-#define CK(x)                                   \
-    do {                                        \
-        cudaError_t e_ = (x);                   \
+#define CK(x)                                        \
+    do {                                             \
+        cudaError_t e_ = (x);                        \
         if (e_ != cudaSuccess) return MGCM_RT_ECUDA; \
     } while (0)
 
@@ -291,37 +323,86 @@ void fill_direct(SegDev &sd, const mgcm_rt_batch_in &in, const mgcm_rt_batch_out
 
 bool red_in_smem(int max_nl) { return col_smem_bytes(max_nl, true) <= SMEM_CAP; }
 
-int fp64_blocks_per_sm(int max_nl) {
-    int nb = 0;
-    const size_t smem = col_smem_bytes(max_nl, red_in_smem(max_nl));
-    cudaFuncSetAttribute(rt_fp64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, rt_fp64_kernel, BLOCK, smem) != cudaSuccess)
-        return 1;
-    return std::max(nb, 1);
+cudaStream_t sync_stream(mgcm_rt_handle *h) {
+    return h->user_stream ? h->user_stream : h->slots[0]->stream;
 }
 
-// Three-kernel FP64 pipeline over chunks of columns (rt_fp64.cu).
-int launch_pipeline(mgcm_rt_handle *h, int total, int max_nl, int &nk) {
-    auto al = [](size_t b) { return (b + 255) / 256 * 256; };
-    const size_t stride = al(col_smem_bytes(max_nl, false));
+// Grows an arena within the handle's HBM budget (arenas never shrink).
+int arena_ensure(mgcm_rt_handle *h, Arena &a, size_t bytes, cudaStream_t s) {
+    if (a.bytes >= bytes) return MGCM_RT_OK;
+    std::lock_guard<std::mutex> lk(h->mem_mu);
+    if (h->used - a.bytes + bytes > h->budget) return MGCM_RT_ENOMEM;
+    if (a.ptr) {
+        CK(cudaStreamSynchronize(s));
+        cudaFree(a.ptr);
+        h->used -= a.bytes;
+    }
+    a.ptr = nullptr;
+    a.bytes = 0;
+    if (cudaMalloc(&a.ptr, bytes) != cudaSuccess) return MGCM_RT_ENOMEM;
+    a.bytes = bytes;
+    h->used += bytes;
+    return MGCM_RT_OK;
+}
+
+int slot_init(Slot &s) {
+    CK(cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking));
+    CK(cudaEventCreate(&s.ev0));
+    CK(cudaEventCreate(&s.ev1));
+    CK(cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming));
+    CK(cudaMallocHost(&s.h_segs, sizeof(SegTable)));
+    CK(cudaMalloc(&s.d_segs, sizeof(SegTable)));
+    CK(cudaMalloc(&s.d_status, 256));
+    CK(cudaMallocHost(&s.h_status, 64));
+    s.d_nsys = reinterpret_cast<unsigned long long *>(reinterpret_cast<char *>(s.d_status) + 128);
+    s.h_nsys = reinterpret_cast<unsigned long long *>(reinterpret_cast<char *>(s.h_status) + 32);
+    *s.h_status = 0;
+    *s.h_nsys = 0;
+    return MGCM_RT_OK;
+}
+
+void slot_free(mgcm_rt_handle *h, Slot &s) {
+    if (s.stream) cudaStreamSynchronize(s.stream);
+    for (Arena *a : {&s.stage, &s.pipe, &s.red})
+        if (a->ptr) {
+            cudaFree(a->ptr);
+            h->used -= a->bytes;
+            a->ptr = nullptr;
+            a->bytes = 0;
+        }
+    if (s.h_segs) cudaFreeHost(s.h_segs);
+    if (s.d_segs) cudaFree(s.d_segs);
+    if (s.d_status) cudaFree(s.d_status);
+    if (s.h_status) cudaFreeHost(s.h_status);
+    if (s.ev0) cudaEventDestroy(s.ev0);
+    if (s.ev1) cudaEventDestroy(s.ev1);
+    if (s.done) cudaEventDestroy(s.done);
+    if (s.stream) cudaStreamDestroy(s.stream);
+}
+
+size_t pipe_bytes_per_col(int max_nl, size_t *stride_out = nullptr) {
+    const size_t stride = (col_smem_bytes(max_nl, false) + 255) / 256 * 256;
+    if (stride_out) *stride_out = stride;
     const size_t row = (size_t)2 * max_nl * sizeof(double);
-    const size_t per_col = stride + NSYS * (sizeof(int) + row + 4 * sizeof(double));
-    const size_t cap = std::min<size_t>(h->budget / 2, (size_t)8 << 30);
-    const int chunk = (int)std::min<size_t>((size_t)total, std::max<size_t>(cap / per_col, 1));
+    return stride + NSYS * (sizeof(int) + row + 4 * sizeof(double));
+}
+
+// Three-kernel pipeline (rt_fp64.cu; MIXED swaps in rt_mixed.cu's solver)
+// over chunks of the columns in the slot's segment table.
+int launch_pipeline(mgcm_rt_handle *h, Slot &sl, cudaStream_t st, int total, int max_nl, int &nk,
+                    int max_chunk) {
+    auto al = [](size_t b) { return (b + 255) / 256 * 256; };
+    size_t stride = 0;
+    const size_t per_col = pipe_bytes_per_col(max_nl, &stride);
+    const size_t row = (size_t)2 * max_nl * sizeof(double);
+    int chunk = std::min(total, max_chunk);
     const size_t n_v = (size_t)chunk * NSYS_V, n_i = (size_t)chunk * NSYS_I;
     const size_t need = al((size_t)chunk * stride) + al(n_v * 4) + al(n_i * 4) + al(n_v * row) +
                         al(n_i * row) + al(n_v * 32) + al(n_i * 32) + 256;
-    if (h->pipe.bytes < need) {
-        if (h->pipe.ptr) {
-            CK(cudaStreamSynchronize(h->stream));
-            cudaFree(h->pipe.ptr);
-        }
-        h->pipe.ptr = nullptr;
-        h->pipe.bytes = 0;
-        if (cudaMalloc(&h->pipe.ptr, need) != cudaSuccess) return MGCM_RT_ENOMEM;
-        h->pipe.bytes = need;
-    }
-    unsigned char *p = static_cast<unsigned char *>(h->pipe.ptr);
+    (void)per_col;
+    int rc = arena_ensure(h, sl.pipe, need, st);
+    if (rc) return rc;
+    unsigned char *p = static_cast<unsigned char *>(sl.pipe.ptr);
     auto take = [&](size_t b) { unsigned char *r = p; p += al(b); return r; };
     unsigned char *blocks = take((size_t)chunk * stride);
     int *list_v = reinterpret_cast<int *>(take(n_v * 4));
@@ -331,87 +412,71 @@ int launch_pipeline(mgcm_rt_handle *h, int total, int max_nl, int &nk) {
     double *sc_v = reinterpret_cast<double *>(take(n_v * 32));
     double *sc_i = reinterpret_cast<double *>(take(n_i * 32));
     unsigned int *counts = reinterpret_cast<unsigned int *>(take(256));
-    // reduce pool: room for a typical column's kept systems in ~48 KB (4 CTAs
-    // per SM); columns with more kept systems sum from global memory
     int pool_rows = (int)std::min<size_t>(NSYS, (48 * 1024) / (16 * (size_t)max_nl + 32));
     if (pool_rows < 24) pool_rows = 0;
     const size_t rsm = reduce_smem_bytes(max_nl, pool_rows);
-    const bool rin = pool_rows > 0;
-    if (h->occ_nl != max_nl) {
-        h->occ_nl = max_nl;
+    const bool mixed = h->cfg.precision == MGCM_RT_MIXED;
+    if (sl.occ_nl != max_nl) {
+        sl.occ_nl = max_nl;
         int a = 1, b = 1, c = 1;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, rt_fp64_screen, BLOCK, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, rt_fp64_screen<false>, BLOCK, 0);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, rt_fp64_solve<false>, 128, 0);
-        cudaFuncSetAttribute(rt_fp64_reduce, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             rin ? (int)rsm : 0);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, rt_fp64_reduce, 160, rin ? rsm : 0);
-        h->occ_screen = std::max(a, 1);
-        h->occ_solve = std::max(b, 1);
-        if (const char *e = std::getenv("MGCM_RT_SOLVE_CTAS_PER_SM")) h->occ_solve = std::max(1, std::atoi(e));
-        h->occ_reduce = std::max(c, 1);
+        cudaFuncSetAttribute(rt_fp64_reduce, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rsm);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, rt_fp64_reduce, 160, rsm);
+        sl.occ_screen = std::max(a, 1);
+        sl.occ_solve = std::max(b, 1);
+        if (const char *e = std::getenv("MGCM_RT_SOLVE_CTAS_PER_SM")) sl.occ_solve = std::max(1, std::atoi(e));
+        sl.occ_reduce = std::max(c, 1);
     }
     for (int c0 = 0; c0 < total; c0 += chunk) {
         const int c1 = std::min(total, c0 + chunk);
-        CK(cudaMemsetAsync(counts, 0, 2 * sizeof(unsigned int), h->stream));
-        const int g1 = std::min(c1 - c0, h->num_sms * h->occ_screen);
-        rt_fp64_screen<<<g1, BLOCK, 0, h->stream>>>(h->d_segs, c0, c1, max_nl, blocks, stride,
-                                                     h->d_kv, h->d_ki, h->d_planck, h->K, list_v,
-                                                     list_i, counts, h->d_status, h->d_nsys);
-        const int g2 = h->num_sms * h->occ_solve;
-        rt_fp64_solve<true><<<g2, 128, 0, h->stream>>>(h->d_segs, c0, max_nl, blocks, stride,
-                                                        h->d_kv, h->K, list_v, counts, fl_v, sc_v);
-        rt_fp64_solve<false><<<g2, 128, 0, h->stream>>>(h->d_segs, c0, max_nl, blocks, stride,
-                                                         h->d_ki, h->K, list_i, counts, fl_i, sc_i);
-        const int g3 = std::min(c1 - c0, h->num_sms * h->occ_reduce);
-        rt_fp64_reduce<<<g3, 160, rin ? rsm : 0, h->stream>>>(h->d_segs, c0, c1, max_nl, blocks,
-                                                               stride, h->K, fl_v, sc_v, fl_i, sc_i,
-                                                               h->d_status, pool_rows);
+        CK(cudaMemsetAsync(counts, 0, 2 * sizeof(unsigned int), st));
+        const int g1 = std::min(c1 - c0, h->num_sms * sl.occ_screen);
+        if (mixed)
+            rt_fp64_screen<true><<<g1, BLOCK, 0, st>>>(sl.d_segs, c0, c1, max_nl, blocks, stride,
+                                                       h->d_kv, h->d_ki, h->d_planck, h->K, list_v,
+                                                       list_i, counts, sl.d_status, sl.d_nsys,
+                                                       h->d_kvf, h->d_kif);
+        else
+            rt_fp64_screen<false><<<g1, BLOCK, 0, st>>>(sl.d_segs, c0, c1, max_nl, blocks, stride,
+                                                        h->d_kv, h->d_ki, h->d_planck, h->K, list_v,
+                                                        list_i, counts, sl.d_status, sl.d_nsys,
+                                                        nullptr, nullptr);
+        const int g2 = h->num_sms * sl.occ_solve;
+        if (mixed) {
+            rt_mixed_solve<true><<<g2, 128, 0, st>>>(sl.d_segs, c0, max_nl, blocks, stride, h->d_kvf,
+                                                     h->d_kv, h->K, list_v, counts, fl_v, sc_v);
+            rt_mixed_solve<false><<<g2, 128, 0, st>>>(sl.d_segs, c0, max_nl, blocks, stride, h->d_kif,
+                                                      h->d_ki, h->K, list_i, counts, fl_i, sc_i);
+        } else {
+            rt_fp64_solve<true><<<g2, 128, 0, st>>>(sl.d_segs, c0, max_nl, blocks, stride, h->d_kv,
+                                                    h->K, list_v, counts, fl_v, sc_v);
+            rt_fp64_solve<false><<<g2, 128, 0, st>>>(sl.d_segs, c0, max_nl, blocks, stride, h->d_ki,
+                                                     h->K, list_i, counts, fl_i, sc_i);
+        }
+        const int g3 = std::min(c1 - c0, h->num_sms * sl.occ_reduce);
+        rt_fp64_reduce<<<g3, 160, rsm, st>>>(sl.d_segs, c0, c1, max_nl, blocks, stride, h->K, fl_v,
+                                             sc_v, fl_i, sc_i, sl.d_status, pool_rows);
         nk += 4;
         CK(cudaGetLastError());
     }
     return MGCM_RT_OK;
 }
 
-// Launches the radiation kernels for the segment table already in h->d_segs.
-int launch_all(mgcm_rt_handle *h, int total, int max_nl, bool validate) {
-    CK(cudaMemsetAsync(h->d_status, 0, sizeof(uint32_t), h->stream));
-    CK(cudaMemsetAsync(h->d_nsys, 0, sizeof(unsigned long long), h->stream));
+// Status words cleared, optional validation, kernels between ev0 and ev1.
+int launch_all(mgcm_rt_handle *h, Slot &sl, cudaStream_t st, int total, int max_nl, int max_chunk) {
+    CK(cudaMemsetAsync(sl.d_status, 0, 256, st));
     int nk = 0;
-    if (validate) {
+    if (h->cfg.validate) {
         const int vb = std::min((total + 255) / 256, h->num_sms * 8);
-        validate_kernel<<<std::max(vb, 1), 256, 0, h->stream>>>(h->d_segs, h->d_status);
+        validate_kernel<<<std::max(vb, 1), 256, 0, st>>>(sl.d_segs, sl.d_status);
         ++nk;
     }
-    CK(cudaEventRecord(h->ev0, h->stream));
-    if (h->cfg.precision == MGCM_RT_FP64) {
-        const int rc = launch_pipeline(h, total, max_nl, nk);
-        if (rc) return rc;
-    } else {
-        const bool in_smem = red_in_smem(max_nl);
-        const size_t smem = col_smem_bytes(max_nl, in_smem);
-        const int grid = std::min(total, h->num_sms * fp64_blocks_per_sm(max_nl));
-        double *red = nullptr;
-        if (!in_smem) {
-            const size_t need = (size_t)grid * red_bytes(max_nl);
-            if (h->red.bytes < need) {
-                if (h->red.ptr) {
-                    CK(cudaStreamSynchronize(h->stream));
-                    cudaFree(h->red.ptr);
-                }
-                h->red.ptr = nullptr;
-                h->red.bytes = 0;
-                if (cudaMalloc(&h->red.ptr, need) != cudaSuccess) return MGCM_RT_ENOMEM;
-                h->red.bytes = need;
-            }
-            red = static_cast<double *>(h->red.ptr);
-        }
-        rt_fp64_kernel<<<grid, BLOCK, smem, h->stream>>>(h->d_segs, h->d_kv, h->d_ki, h->d_planck,
-                                                         h->K, max_nl, h->d_status, h->d_nsys, red);
-        ++nk;
-    }
-    CK(cudaGetLastError());
-    CK(cudaEventRecord(h->ev1, h->stream));
-    h->stats.kernels = nk;
+    CK(cudaEventRecord(sl.ev0, st));
+    const int rc = launch_pipeline(h, sl, st, total, max_nl, nk, max_chunk);
+    if (rc) return rc;
+    CK(cudaEventRecord(sl.ev1, st));
+    sl.kernels = nk;
     return MGCM_RT_OK;
 }
 
@@ -423,132 +488,291 @@ int status_to_code(uint32_t st) {
     return MGCM_RT_OK;
 }
 
-int finish(mgcm_rt_handle *h, long long cols) {
-    CK(cudaStreamSynchronize(h->stream));
-    uint32_t st = 0;
-    unsigned long long ns = 0;
-    CK(cudaMemcpy(&st, h->d_status, sizeof(st), cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(&ns, h->d_nsys, sizeof(ns), cudaMemcpyDeviceToHost));
-    float ms = 0.f;
-    cudaEventElapsedTime(&ms, h->ev0, h->ev1);
-    h->stats.gpu_ms = ms;
-    h->stats.columns = cols;
-    h->stats.systems = (long long)ns;
-    h->stats.status = (int)st;
-    return status_to_code(st);
-}
-
-int ensure_stage(mgcm_rt_handle *h, size_t bytes) {
-    if (h->stage.bytes >= bytes) return MGCM_RT_OK;
-    if (bytes > h->budget) return MGCM_RT_ENOMEM;
-    if (h->stage.ptr) cudaFree(h->stage.ptr);
-    h->stage.ptr = nullptr;
-    h->stage.bytes = 0;
-    if (cudaMalloc(&h->stage.ptr, bytes) != cudaSuccess) return MGCM_RT_ENOMEM;
-    h->stage.bytes = bytes;
+// Copies the slot's status words to pinned host memory on its stream.
+int post_status(Slot &sl, cudaStream_t st) {
+    CK(cudaMemcpyAsync(sl.h_status, sl.d_status, 4, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(sl.h_nsys, sl.d_nsys, 8, cudaMemcpyDeviceToHost, st));
     return MGCM_RT_OK;
 }
 
-// Runs nbatch segments (all host or all device pointers); synchronous unless
-// async (device pointers only), in which case the caller later calls finish().
-int run_segments(mgcm_rt_handle *h, int nbatch, const mgcm_rt_batch_in *in,
-                 mgcm_rt_batch_out *out, bool async = false) {
-    if (nbatch < 1 || nbatch > MAX_SEGS) return MGCM_RT_EINVAL;
-    const auto t0 = std::chrono::steady_clock::now();
-    const int kind = in[0].device_ptrs ? 1 : 0;
-    if (async && !kind) return MGCM_RT_EINVAL;
-    if (h->pending) {   // a previous enqueue not yet synced: its segment table is in use
-        const int rc = finish(h, h->pending_cols);
-        h->pending = false;
+// Issues one job on a slot: staging of host arrays (column range [c0,c1) of
+// batch in/out), the kernels and the copies back; records sl.done.
+int issue_job(mgcm_rt_handle *h, Slot &sl, cudaStream_t st, const mgcm_rt_batch_in &in,
+              const mgcm_rt_batch_out &out, int c0, int c1) {
+    const Sizes z = sizes_of(in);
+    const size_t n = (size_t)(c1 - c0);
+    SegDev sd{};
+    sd.ncol = (int)n;
+    sd.L = z.L;
+    sd.col0 = 0;
+    sd.ptrop = in.ptrop;
+    std::vector<ArrSpec> arrs;
+    if (in.device_ptrs) {
+        fill_direct(sd, in, out);
+        // shift every per-column pointer to the job's first column
+        arrs = arrays_of(in, out, z, sd);
+        for (auto &a : arrs) *a.seg_field = const_cast<double *>(a.src ? a.src : a.dst) + (size_t)c0 * a.per_col;
+        sd.sigma = in.sigma;
+        sd.sol = in.sol;
+    } else {
+        arrs = arrays_of(in, out, z, sd);
+        size_t bytes = ((z.lev + 8) * 8 + 255) / 256 * 256;
+        for (const auto &a : arrs) bytes += ((a.per_col * n * 8 + 255) / 256) * 256;
+        const int rc = arena_ensure(h, sl.stage, bytes, st);
         if (rc) return rc;
+        char *base = static_cast<char *>(sl.stage.ptr);
+        size_t off = 0;
+        for (auto &a : arrs) {
+            double *d = reinterpret_cast<double *>(base + off);
+            off += ((a.per_col * n * 8 + 255) / 256) * 256;
+            *a.seg_field = d;
+            a.dev = d;
+            if (a.dir != 1)
+                CK(cudaMemcpyAsync(d, a.src + (size_t)c0 * a.per_col, a.per_col * n * 8,
+                                   cudaMemcpyHostToDevice, st));
+        }
+        double *ds = reinterpret_cast<double *>(base + off);
+        CK(cudaMemcpyAsync(ds, in.sigma, z.lev * 8, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(ds + z.lev, in.sol, 7 * 8, cudaMemcpyHostToDevice, st));
+        sd.sigma = ds;
+        sd.sol = ds + z.lev;
     }
-    SegTable &tab = *h->h_segs;
+    SegTable &tab = *sl.h_segs;
+    tab.nseg = 1;
+    tab.total_cols = (int)n;
+    tab.seg[0] = sd;
+    CK(cudaMemcpyAsync(sl.d_segs, sl.h_segs, offsetof(SegTable, seg) + sizeof(SegDev),
+                       cudaMemcpyHostToDevice, st));
+    int rc = launch_all(h, sl, st, (int)n, z.nl, 1 << 30);
+    if (rc) return rc;
+    if (!in.device_ptrs)
+        for (auto &a : arrs)
+            if (a.dir != 0)
+                CK(cudaMemcpyAsync(a.dst + (size_t)c0 * a.per_col, a.dev, a.per_col * n * 8,
+                                   cudaMemcpyDeviceToHost, st));
+    rc = post_status(sl, st);
+    if (rc) return rc;
+    CK(cudaEventRecord(sl.done, st));
+    return MGCM_RT_OK;
+}
+
+// Synchronous batch of device-pointer segments on slot 0 (async: leave pending).
+int run_device(mgcm_rt_handle *h, int nbatch, const mgcm_rt_batch_in *in, mgcm_rt_batch_out *out,
+               bool async) {
+    Slot &sl = *h->slots[0];
+    cudaStream_t st = sync_stream(h);
+    SegTable &tab = *sl.h_segs;
     tab.nseg = 0;
     int total = 0, max_nl = 1;
-    size_t stage_bytes = 0;
     for (int b = 0; b < nbatch; ++b) {
-        const int rc = check_args(h, &in[b], &out[b]);
-        if (rc) return rc;
-        if ((in[b].device_ptrs ? 1 : 0) != kind) return MGCM_RT_EINVAL;
         const Sizes z = sizes_of(in[b]);
         if (z.ncol == 0) continue;
-        if ((long long)total + (long long)z.ncol > 0x7fffffff) return MGCM_RT_EINVAL;
+        if ((long long)total + (long long)z.ncol > 0x7fffff) return MGCM_RT_EINVAL;
         SegDev sd{};
-        const auto arrs = arrays_of(in[b], out[b], z, sd);
-        for (const auto &a : arrs) stage_bytes += ((a.per_col * z.ncol * 8 + 255) / 256) * 256;
-        stage_bytes += ((z.lev + 8) * 8 + 255) / 256 * 256;   // sigma + sol
+        sd.ncol = (int)z.ncol;
+        sd.L = z.L;
+        sd.col0 = total;
+        sd.ptrop = in[b].ptrop;
+        fill_direct(sd, in[b], out[b]);
+        sd.sigma = in[b].sigma;
+        sd.sol = in[b].sol;
+        tab.seg[tab.nseg++] = sd;
         max_nl = std::max(max_nl, z.nl);
         total += (int)z.ncol;
     }
     if (total == 0) return MGCM_RT_OK;
-    if (!kind) {
-        const int rc = ensure_stage(h, stage_bytes);
-        if (rc) return rc;
-    }
-    char *base = static_cast<char *>(h->stage.ptr);
-    size_t off = 0;
-    int col0 = 0;
-    std::vector<std::pair<std::vector<ArrSpec>, size_t>> pending;   // for D2H
+    tab.total_cols = total;
+    CK(cudaMemcpyAsync(sl.d_segs, sl.h_segs, sizeof(SegTable), cudaMemcpyHostToDevice, st));
+    // pipeline chunk: bounded by a quarter of the budget
+    const size_t per_col = pipe_bytes_per_col(max_nl);
+    const int chunk = (int)std::max<size_t>(1, std::min<size_t>(total, (h->budget / 4) / per_col));
+    int rc = launch_all(h, sl, st, total, max_nl, chunk);
+    if (rc) return rc;
+    rc = post_status(sl, st);
+    if (rc) return rc;
+    h->pending = true;
+    h->pending_cols = total;
+    if (async) return MGCM_RT_OK;
+    CK(cudaStreamSynchronize(st));
+    h->pending = false;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, sl.ev0, sl.ev1);
+    h->stats.gpu_ms = ms;
+    h->stats.columns = total;
+    h->stats.systems = (long long)*sl.h_nsys;
+    h->stats.status = (int)*sl.h_status;
+    h->stats.kernels = sl.kernels;
+    return status_to_code(*sl.h_status);
+}
+
+int finish_pending(mgcm_rt_handle *h) {
+    if (!h->pending) return MGCM_RT_OK;
+    Slot &sl = *h->slots[0];
+    CK(cudaStreamSynchronize(sync_stream(h)));
+    h->pending = false;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, sl.ev0, sl.ev1);
+    h->stats.gpu_ms = ms;
+    h->stats.columns = h->pending_cols;
+    h->stats.systems = (long long)*sl.h_nsys;
+    h->stats.status = (int)*sl.h_status;
+    h->stats.kernels = sl.kernels;
+    return status_to_code(*sl.h_status);
+}
+
+// Synchronous batch of host-pointer segments: jobs alternate between the two
+// synchronous slots, forked from and joined back into the caller's stream.
+int run_host(mgcm_rt_handle *h, int nbatch, const mgcm_rt_batch_in *in, mgcm_rt_batch_out *out) {
+    cudaStream_t ust = sync_stream(h);
+    CK(cudaEventRecord(h->fork, ust));
+    for (auto &s : h->slots) CK(cudaStreamWaitEvent(s->stream, h->fork, 0));
+    uint32_t acc = 0;
+    long long cols = 0, systems = 0;
+    int nk = 0, k = 0;
+    bool used[2] = {false, false};
     for (int b = 0; b < nbatch; ++b) {
         const Sizes z = sizes_of(in[b]);
-        if (z.ncol == 0) continue;
-        SegDev sd{};
-        sd.ncol = (int)z.ncol;
-        sd.L = z.L;
-        sd.col0 = col0;
-        sd.ptrop = in[b].ptrop;
-        if (kind) {
-            fill_direct(sd, in[b], out[b]);
-            sd.sigma = in[b].sigma;
-            sd.sol = in[b].sol;
-        } else {
-            auto arrs = arrays_of(in[b], out[b], z, sd);
-            for (auto &a : arrs) {
-                double *d = reinterpret_cast<double *>(base + off);
-                off += ((a.per_col * z.ncol * 8 + 255) / 256) * 256;
-                *a.seg_field = d;
-                a.dev = d;
-                if (a.dir != 1)
-                    CK(cudaMemcpyAsync(d, a.src, a.per_col * z.ncol * 8, cudaMemcpyHostToDevice, h->stream));
+        for (int c0 = 0; c0 < (int)z.ncol; c0 += SYNC_JOB_COLS, ++k) {
+            const int c1 = std::min((int)z.ncol, c0 + SYNC_JOB_COLS);
+            Slot &sl = *h->slots[k & 1];
+            if (used[k & 1]) {   // the slot's previous job must finish before its buffers are reused
+                CK(cudaEventSynchronize(sl.done));
+                acc |= *sl.h_status;
+                systems += (long long)*sl.h_nsys;
             }
-            double *ds = reinterpret_cast<double *>(base + off);
-            off += ((z.lev + 8) * 8 + 255) / 256 * 256;
-            CK(cudaMemcpyAsync(ds, in[b].sigma, z.lev * 8, cudaMemcpyHostToDevice, h->stream));
-            CK(cudaMemcpyAsync(ds + z.lev, in[b].sol, 7 * 8, cudaMemcpyHostToDevice, h->stream));
-            sd.sigma = ds;
-            sd.sol = ds + z.lev;
-            pending.push_back({arrs, z.ncol});
+            const int rc = issue_job(h, sl, sl.stream, in[b], out[b], c0, c1);
+            if (rc) return rc;
+            used[k & 1] = true;
+            nk += sl.kernels;
+            cols += c1 - c0;
         }
-        tab.seg[tab.nseg++] = sd;
-        col0 += (int)z.ncol;
     }
-    tab.total_cols = total;
-    CK(cudaMemcpyAsync(h->d_segs, h->h_segs, sizeof(SegTable), cudaMemcpyHostToDevice, h->stream));
-    int rc = launch_all(h, total, max_nl, h->cfg.validate != 0);
+    for (int i = 0; i < 2; ++i) {
+        Slot &sl = *h->slots[i];
+        if (used[i]) {
+            CK(cudaEventSynchronize(sl.done));
+            acc |= *sl.h_status;
+            systems += (long long)*sl.h_nsys;
+        }
+    }
+    CK(cudaEventRecord(h->join0, h->slots[0]->stream));
+    CK(cudaEventRecord(h->join1, h->slots[1]->stream));
+    CK(cudaStreamWaitEvent(ust, h->join0, 0));
+    CK(cudaStreamWaitEvent(ust, h->join1, 0));
+    float ms = 0.f;
+    if (used[0]) cudaEventElapsedTime(&ms, h->slots[0]->ev0, h->slots[0]->ev1);
+    h->stats.gpu_ms = ms;
+    h->stats.columns = cols;
+    h->stats.systems = systems;
+    h->stats.status = (int)acc;
+    h->stats.kernels = nk;
+    return status_to_code(acc);
+}
+
+int run_batches(mgcm_rt_handle *h, int nbatch, const mgcm_rt_batch_in *in, mgcm_rt_batch_out *out,
+                bool async) {
+    if (nbatch < 1 || nbatch > MAX_SEGS) return MGCM_RT_EINVAL;
+    const auto t0 = std::chrono::steady_clock::now();
+    const int kind = in[0].device_ptrs ? 1 : 0;
+    if (async && !kind) return MGCM_RT_EINVAL;
+    for (int b = 0; b < nbatch; ++b) {
+        const int rc = check_args(h, &in[b], &out[b]);
+        if (rc) return rc;
+        if ((in[b].device_ptrs ? 1 : 0) != kind) return MGCM_RT_EINVAL;
+    }
+    int rc = finish_pending(h);
     if (rc) return rc;
-    if (!kind) {
-        for (size_t i = 0; i < pending.size(); ++i)
-            for (auto &a : pending[i].first)
-                if (a.dir != 0)
-                    CK(cudaMemcpyAsync(a.dst, a.dev, a.per_col * pending[i].second * 8,
-                                       cudaMemcpyDeviceToHost, h->stream));
-    }
-    if (async) {
-        h->pending = true;
-        h->pending_cols = total;
-        return MGCM_RT_OK;
-    }
-    rc = finish(h, total);
+    rc = kind ? run_device(h, nbatch, in, out, async) : run_host(h, nbatch, in, out);
     h->stats.total_ms =
         std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     return rc;
+}
+
+// ---------------------------------------------------------------- serving
+void finish_job(mgcm_rt_handle *h, Slot &sl) {
+    std::shared_ptr<Request> r = sl.job.req;
+    const int code = status_to_code(*sl.h_status);
+    sl.busy = false;
+    sl.job = Job{};
+    std::lock_guard<std::mutex> lk(h->qmu);
+    if (code && !r->status) r->status = code;
+    if (--r->jobs_left == 0) {
+        r->done = true;
+        r->t_done = std::chrono::steady_clock::now();
+        h->dcv.notify_all();
+    }
+}
+
+void fail_job(mgcm_rt_handle *h, Job &j, int code) {
+    std::lock_guard<std::mutex> lk(h->qmu);
+    if (!j.req->status) j.req->status = code;
+    if (--j.req->jobs_left == 0) {
+        j.req->done = true;
+        j.req->t_done = std::chrono::steady_clock::now();
+        h->dcv.notify_all();
+    }
+}
+
+void worker_main(mgcm_rt_handle *h) {
+    cudaSetDevice(h->device);
+    for (;;) {
+        bool any_busy = false;
+        for (auto &s : h->sslots)
+            if (s->busy) {
+                if (cudaEventQuery(s->done) == cudaSuccess) finish_job(h, *s);
+                else any_busy = true;
+            }
+        for (;;) {   // admit jobs onto free slots
+            Job j;
+            {
+                std::lock_guard<std::mutex> lk(h->qmu);
+                if (h->jobs.empty()) break;
+                j = h->jobs.front();
+            }
+            Slot *free_slot = nullptr;
+            for (auto &s : h->sslots)
+                if (!s->busy) { free_slot = s.get(); break; }
+            if (!free_slot && (int)h->sslots.size() < SERVE_SLOTS) {
+                auto s = std::make_unique<Slot>();
+                if (slot_init(*s) == MGCM_RT_OK) {
+                    h->sslots.push_back(std::move(s));
+                    free_slot = h->sslots.back().get();
+                }
+            }
+            if (!free_slot) break;
+            {
+                std::lock_guard<std::mutex> lk(h->qmu);
+                h->jobs.pop_front();
+            }
+            const int rc = issue_job(h, *free_slot, free_slot->stream, j.req->in[j.seg], j.req->out[j.seg],
+                                     j.c0, j.c1);
+            if (rc == MGCM_RT_ENOMEM && any_busy) {   // admitted later, when memory frees up
+                std::lock_guard<std::mutex> lk(h->qmu);
+                h->jobs.push_front(j);
+                break;
+            }
+            if (rc) {
+                fail_job(h, j, rc);
+                continue;
+            }
+            free_slot->busy = true;
+            free_slot->job = j;
+            any_busy = true;
+        }
+        std::unique_lock<std::mutex> lk(h->qmu);
+        if (h->stop && h->jobs.empty() && !any_busy) return;
+        if (any_busy)
+            h->qcv.wait_for(lk, std::chrono::microseconds(50));
+        else
+            h->qcv.wait(lk, [&] { return h->stop || !h->jobs.empty(); });
+    }
 }
 
 }  // namespace
 
 extern "C" {
 
-const char *mgcm_rt_version(void) { return "mgcm-rt-b200 0.1 (Legacy Mars GCM v24 radiation)"; }
+const char *mgcm_rt_version(void) { return "mgcm-rt-b200 0.2 (Legacy Mars GCM v24 radiation)"; }
 
 const char *mgcm_rt_strerror(int s) {
     switch (s) {
@@ -584,7 +808,7 @@ mgcm_rt_handle *mgcm_rt_create(const mgcm_rt_config *cfg, const char *data_dir, 
     if (!status) status = &dummy;
     if (!cfg || !data_dir) { *status = MGCM_RT_EINVAL; return nullptr; }
     if (cfg->max_layers < 1 || cfg->max_layers > MGCM_RT_MAX_LAYERS) { *status = MGCM_RT_ELAYERS; return nullptr; }
-    if (cfg->precision != MGCM_RT_FP64) { *status = MGCM_RT_EINVAL; return nullptr; }
+    if (cfg->precision != MGCM_RT_FP64 && cfg->precision != MGCM_RT_MIXED) { *status = MGCM_RT_EINVAL; return nullptr; }
     auto h = std::make_unique<mgcm_rt_handle>();
     h->cfg = *cfg;
     if (load_tables(data_dir, h->host)) { *status = MGCM_RT_EIO; return nullptr; }
@@ -594,10 +818,14 @@ mgcm_rt_handle *mgcm_rt_create(const mgcm_rt_config *cfg, const char *data_dir, 
     if (cudaGetDeviceProperties(&prop, h->device) != cudaSuccess) { *status = MGCM_RT_ECUDA; return nullptr; }
     h->num_sms = prop.multiProcessorCount;
     auto fail = [&](int code) { mgcm_rt_destroy(h.release()); *status = code; return nullptr; };
-    if (cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking) != cudaSuccess) return fail(MGCM_RT_ECUDA);
-    h->stream = h->own_stream;
-    if (cudaEventCreate(&h->ev0) != cudaSuccess || cudaEventCreate(&h->ev1) != cudaSuccess) return fail(MGCM_RT_ECUDA);
-    // constants
+    for (int i = 0; i < 2; ++i) {
+        h->slots.push_back(std::make_unique<Slot>());
+        if (slot_init(*h->slots.back())) return fail(MGCM_RT_ECUDA);
+    }
+    if (cudaEventCreateWithFlags(&h->fork, cudaEventDisableTiming) ||
+        cudaEventCreateWithFlags(&h->join0, cudaEventDisableTiming) ||
+        cudaEventCreateWithFlags(&h->join1, cudaEventDisableTiming))
+        return fail(MGCM_RT_ECUDA);
     RtConst &K = h->K;
     std::memcpy(K.tauray, h->host.tauray, sizeof(K.tauray));
     std::memcpy(K.fzerov, h->host.fzerov, sizeof(K.fzerov));
@@ -607,16 +835,16 @@ mgcm_rt_handle *mgcm_rt_create(const mgcm_rt_config *cfg, const char *data_dir, 
     std::memcpy(K.pfgasref, h->host.pfgasref, sizeof(K.pfgasref));
     std::memcpy(K.plimit, h->host.plimit, sizeof(K.plimit));
     std::memcpy(K.wrefh2o, h->host.wrefh2o, sizeof(K.wrefh2o));
-    // device tables
     std::vector<double> kv, ki;
     gauss_fastest(h->host, kv, ki);
-    std::vector<float> kvf(kv.begin(), kv.end()), kif(ki.begin(), ki.end());
+    // FP32 tables hold Cmk*k (optical depth per mbar): k itself reaches 1e-49,
+    // below the FP32 range (code/optcv.f90:241-242, U = Cmk*DPR)
+    std::vector<float> kvf(kv.size()), kif(ki.size());
+    for (size_t q = 0; q < kv.size(); ++q) kvf[q] = (float)(3.51e22 * kv[q]);
+    for (size_t q = 0; q < ki.size(); ++q) kif[q] = (float)(3.51e22 * ki[q]);
     if (cudaMalloc(&h->d_kv, kv.size() * 8) || cudaMalloc(&h->d_ki, ki.size() * 8) ||
         cudaMalloc(&h->d_kvf, kvf.size() * 4) || cudaMalloc(&h->d_kif, kif.size() * 4) ||
-        cudaMalloc(&h->d_planck, h->host.planckir.size() * 8) ||
-        cudaMalloc(&h->d_status, 64) || cudaMalloc(&h->d_nsys, 64) ||
-        cudaMalloc(&h->d_segs, sizeof(SegTable)) ||
-        cudaMallocHost(&h->h_segs, sizeof(SegTable)))
+        cudaMalloc(&h->d_planck, h->host.planckir.size() * 8))
         return fail(MGCM_RT_ENOMEM);
     if (cudaMemcpy(h->d_kv, kv.data(), kv.size() * 8, cudaMemcpyHostToDevice) ||
         cudaMemcpy(h->d_ki, ki.data(), ki.size() * 8, cudaMemcpyHostToDevice) ||
@@ -634,23 +862,24 @@ mgcm_rt_handle *mgcm_rt_create(const mgcm_rt_config *cfg, const char *data_dir, 
 void mgcm_rt_destroy(mgcm_rt_handle *h) {
     if (!h) return;
     cudaSetDevice(h->device);
-    if (h->stream) cudaStreamSynchronize(h->stream);
-    h->stream = h->own_stream;
+    if (h->worker.joinable()) {
+        {
+            std::lock_guard<std::mutex> lk(h->qmu);
+            h->stop = true;
+        }
+        h->qcv.notify_all();
+        h->worker.join();
+    }
+    for (auto &s : h->sslots) slot_free(h, *s);
+    for (auto &s : h->slots) slot_free(h, *s);
     cudaFree(h->d_kv);
     cudaFree(h->d_ki);
     cudaFree(h->d_kvf);
     cudaFree(h->d_kif);
     cudaFree(h->d_planck);
-    cudaFree(h->d_status);
-    cudaFree(h->d_nsys);
-    cudaFree(h->d_segs);
-    if (h->h_segs) cudaFreeHost(h->h_segs);
-    if (h->stage.ptr) cudaFree(h->stage.ptr);
-    if (h->red.ptr) cudaFree(h->red.ptr);
-    if (h->pipe.ptr) cudaFree(h->pipe.ptr);
-    if (h->ev0) cudaEventDestroy(h->ev0);
-    if (h->ev1) cudaEventDestroy(h->ev1);
-    if (h->own_stream) cudaStreamDestroy(h->own_stream);
+    if (h->fork) cudaEventDestroy(h->fork);
+    if (h->join0) cudaEventDestroy(h->join0);
+    if (h->join1) cudaEventDestroy(h->join1);
     delete h;
 }
 
@@ -658,7 +887,7 @@ int mgcm_rt_run(mgcm_rt_handle *h, const mgcm_rt_batch_in *in, mgcm_rt_batch_out
     if (!h || !in || !out) return MGCM_RT_EINVAL;
     std::lock_guard<std::mutex> lk(h->mu);
     if (cudaSetDevice(h->device) != cudaSuccess) return MGCM_RT_ECUDA;
-    return run_segments(h, 1, in, out);
+    return run_batches(h, 1, in, out, false);
 }
 
 int mgcm_rt_run_multi(mgcm_rt_handle *h, int nbatch, const mgcm_rt_batch_in *in,
@@ -666,14 +895,14 @@ int mgcm_rt_run_multi(mgcm_rt_handle *h, int nbatch, const mgcm_rt_batch_in *in,
     if (!h || !in || !out) return MGCM_RT_EINVAL;
     std::lock_guard<std::mutex> lk(h->mu);
     if (cudaSetDevice(h->device) != cudaSuccess) return MGCM_RT_ECUDA;
-    return run_segments(h, nbatch, in, out);
+    return run_batches(h, nbatch, in, out, false);
 }
 
 int mgcm_rt_enqueue(mgcm_rt_handle *h, const mgcm_rt_batch_in *in, mgcm_rt_batch_out *out) {
     if (!h || !in || !out) return MGCM_RT_EINVAL;
     std::lock_guard<std::mutex> lk(h->mu);
     if (cudaSetDevice(h->device) != cudaSuccess) return MGCM_RT_ECUDA;
-    return run_segments(h, 1, in, out, true);
+    return run_batches(h, 1, in, out, true);
 }
 
 int mgcm_rt_sync(mgcm_rt_handle *h) {
@@ -681,23 +910,19 @@ int mgcm_rt_sync(mgcm_rt_handle *h) {
     std::lock_guard<std::mutex> lk(h->mu);
     if (cudaSetDevice(h->device) != cudaSuccess) return MGCM_RT_ECUDA;
     if (!h->pending) {
-        CK(cudaStreamSynchronize(h->stream));
+        CK(cudaStreamSynchronize(sync_stream(h)));
         return MGCM_RT_OK;
     }
-    h->pending = false;
-    return finish(h, h->pending_cols);
+    return finish_pending(h);
 }
 
 int mgcm_rt_set_stream(mgcm_rt_handle *h, void *cuda_stream) {
     if (!h) return MGCM_RT_EINVAL;
     std::lock_guard<std::mutex> lk(h->mu);
-    if (h->pending) {
-        h->pending = false;
-        const int rc = finish(h, h->pending_cols);
-        if (rc) return rc;
-    }
-    CK(cudaStreamSynchronize(h->stream));
-    h->stream = cuda_stream ? static_cast<cudaStream_t>(cuda_stream) : h->own_stream;
+    const int rc = finish_pending(h);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(sync_stream(h)));
+    h->user_stream = static_cast<cudaStream_t>(cuda_stream);
     return MGCM_RT_OK;
 }
 
@@ -715,41 +940,65 @@ int mgcm_rt_dsolflux(mgcm_rt_handle *h, int ncol, int device_ptrs, const double 
     if (ncol == 0) return MGCM_RT_OK;
     std::lock_guard<std::mutex> lk(h->mu);
     if (cudaSetDevice(h->device) != cudaSuccess) return MGCM_RT_ECUDA;
+    int rc = finish_pending(h);
+    if (rc) return rc;
+    Slot &sl = *h->slots[0];
+    cudaStream_t st = sync_stream(h);
     const double *ds = sol, *da = acosz, *dd = detau, *dn = dndiffv;
     double *dout = dnvflux;
     if (!device_ptrs) {
         const size_t n = (size_t)ncol;
         const size_t bytes = 8 * (8 + n + 119 * n + n + n) + 5 * 256;
-        const int rc = ensure_stage(h, bytes);
+        rc = arena_ensure(h, sl.stage, bytes, st);
         if (rc) return rc;
-        char *b = static_cast<char *>(h->stage.ptr);
-        double *p = reinterpret_cast<double *>(b);
+        double *p = static_cast<double *>(sl.stage.ptr);
         double *pa = p + 8, *pd = pa + n, *pn = pd + 119 * n, *po = pn + n;
-        CK(cudaMemcpyAsync(p, sol, 7 * 8, cudaMemcpyHostToDevice, h->stream));
-        CK(cudaMemcpyAsync(pa, acosz, n * 8, cudaMemcpyHostToDevice, h->stream));
-        CK(cudaMemcpyAsync(pd, detau, 119 * n * 8, cudaMemcpyHostToDevice, h->stream));
-        CK(cudaMemcpyAsync(pn, dndiffv, n * 8, cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemcpyAsync(p, sol, 7 * 8, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(pa, acosz, n * 8, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(pd, detau, 119 * n * 8, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(pn, dndiffv, n * 8, cudaMemcpyHostToDevice, st));
         ds = p; da = pa; dd = pd; dn = pn; dout = po;
     }
-    rt_dsolflux_kernel<<<(ncol + 127) / 128, 128, 0, h->stream>>>(ncol, ds, da, dd, dn, dout, h->K);
+    rt_dsolflux_kernel<<<(ncol + 127) / 128, 128, 0, st>>>(ncol, ds, da, dd, dn, dout, h->K);
     CK(cudaGetLastError());
-    if (!device_ptrs) CK(cudaMemcpyAsync(dnvflux, dout, (size_t)ncol * 8, cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaStreamSynchronize(h->stream));
+    if (!device_ptrs) CK(cudaMemcpyAsync(dnvflux, dout, (size_t)ncol * 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
     return MGCM_RT_OK;
 }
 
-// Serving: a submitted batch runs at once on the handle's stream; wait()
-// collects its status.
 int mgcm_rt_submit(mgcm_rt_handle *h, const mgcm_rt_batch_in *in, mgcm_rt_batch_out *out,
                    long long *ticket) {
     if (!h || !in || !out || !ticket) return MGCM_RT_EINVAL;
-    const int rc = mgcm_rt_run(h, in, out);
-    std::lock_guard<std::mutex> lk(h->qmu);
+    const int rc = check_args(h, in, out);
+    if (rc) return rc;
     auto r = std::make_shared<Request>();
-    r->status = rc;
-    r->done = true;
+    r->in.push_back(*in);
+    r->out.push_back(*out);
+    r->t_submit = std::chrono::steady_clock::now();
+    const int ncol = in->ncol;
+    std::lock_guard<std::mutex> lk(h->qmu);
+    if (h->jobs.size() > 100000) return MGCM_RT_EBUSY;
+    if (!h->worker.joinable()) {
+        h->stop = false;
+        h->worker = std::thread(worker_main, h);
+    }
     *ticket = h->next_ticket++;
     h->reqs[*ticket] = r;
+    if (ncol == 0) {
+        r->done = true;
+        r->t_done = r->t_submit;
+        return MGCM_RT_OK;
+    }
+    for (int c0 = 0; c0 < ncol; c0 += SERVE_JOB_COLS) {
+        Job j;
+        j.req = r;
+        j.seg = 0;
+        j.c0 = c0;
+        j.c1 = std::min(ncol, c0 + SERVE_JOB_COLS);
+        ++r->jobs_left;
+        h->jobs.push_back(j);
+    }
+    h->qcv.notify_all();
     return MGCM_RT_OK;
 }
 
@@ -764,13 +1013,17 @@ int mgcm_rt_poll(mgcm_rt_handle *h, long long ticket) {
 
 int mgcm_rt_wait(mgcm_rt_handle *h, long long ticket, double timeout_s) {
     if (!h) return MGCM_RT_EINVAL;
-    (void)timeout_s;
-    std::lock_guard<std::mutex> lk(h->qmu);
+    std::unique_lock<std::mutex> lk(h->qmu);
     auto it = h->reqs.find(ticket);
     if (it == h->reqs.end()) return MGCM_RT_ENOTFOUND;
-    const int st = it->second->status;
-    h->reqs.erase(it);
-    return st;
+    std::shared_ptr<Request> r = it->second;
+    if (timeout_s < 0) {
+        h->dcv.wait(lk, [&] { return r->done; });
+    } else if (!h->dcv.wait_for(lk, std::chrono::duration<double>(timeout_s), [&] { return r->done; })) {
+        return MGCM_RT_ETIMEOUT;
+    }
+    h->reqs.erase(ticket);
+    return r->status;
 }
 }
 
@@ -812,11 +1065,10 @@ extern "C" int mgcm_rt_run_noalloc(mgcm_rt_handle *h, const mgcm_rt_batch_in *in
     int rc = check_args(h, in, out);
     if (rc) return rc;
     if (in->ncol == 0) return MGCM_RT_OK;
-    if (h->pending) {
-        h->pending = false;
-        rc = finish(h, h->pending_cols);
-        if (rc) return rc;
-    }
+    rc = finish_pending(h);
+    if (rc) return rc;
+    Slot &sl = *h->slots[0];
+    cudaStream_t stream = sync_stream(h);
     unsigned char *scr = nullptr;
     rc = noalloc_scratch(h->device, &scr);
     if (rc) return rc;
@@ -836,7 +1088,7 @@ extern "C" int mgcm_rt_run_noalloc(mgcm_rt_handle *h, const mgcm_rt_batch_in *in
     const size_t want = (size_t)h->num_sms * (size_t)std::max(nb, 1);
     const int grid = (int)std::min({(size_t)z.ncol, want, nslab});
     // descriptor: header + one segment, staged through the handle's pinned buffer
-    SegTable &tab = *h->h_segs;
+    SegTable &tab = *sl.h_segs;
     tab.nseg = 1;
     tab.total_cols = (int)z.ncol;
     SegDev sd{};
@@ -852,22 +1104,22 @@ extern "C" int mgcm_rt_run_noalloc(mgcm_rt_handle *h, const mgcm_rt_batch_in *in
     uint32_t *d_status = reinterpret_cast<uint32_t *>(scr + NOALLOC_HDR - 256);
     unsigned long long *d_nsys = reinterpret_cast<unsigned long long *>(scr + NOALLOC_HDR - 128);
     double *d_red = reinterpret_cast<double *>(scr + NOALLOC_HDR);
-    CK(cudaMemcpyAsync(d_tab, h->h_segs, offsetof(SegTable, seg) + sizeof(SegDev),
-                       cudaMemcpyHostToDevice, h->stream));
-    CK(cudaMemsetAsync(d_status, 0, sizeof(uint32_t), h->stream));
-    CK(cudaMemsetAsync(d_nsys, 0, sizeof(unsigned long long), h->stream));
-    CK(cudaEventRecord(h->ev0, h->stream));
-    rt_fp64_kernel<<<grid, BLOCK, smem, h->stream>>>(d_tab, h->d_kv, h->d_ki, h->d_planck, h->K,
+    CK(cudaMemcpyAsync(d_tab, sl.h_segs, offsetof(SegTable, seg) + sizeof(SegDev),
+                       cudaMemcpyHostToDevice, stream));
+    CK(cudaMemsetAsync(d_status, 0, sizeof(uint32_t), stream));
+    CK(cudaMemsetAsync(d_nsys, 0, sizeof(unsigned long long), stream));
+    CK(cudaEventRecord(sl.ev0, stream));
+    rt_fp64_kernel<<<grid, BLOCK, smem, stream>>>(d_tab, h->d_kv, h->d_ki, h->d_planck, h->K,
                                                      max_nl, d_status, d_nsys, d_red);
     CK(cudaGetLastError());
-    CK(cudaEventRecord(h->ev1, h->stream));
-    CK(cudaStreamSynchronize(h->stream));
+    CK(cudaEventRecord(sl.ev1, stream));
+    CK(cudaStreamSynchronize(stream));
     uint32_t st = 0;
     unsigned long long ns = 0;
     CK(cudaMemcpy(&st, d_status, sizeof(st), cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(&ns, d_nsys, sizeof(ns), cudaMemcpyDeviceToHost));
     float ms = 0.f;
-    cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+    cudaEventElapsedTime(&ms, sl.ev0, sl.ev1);
     h->stats.gpu_ms = ms;
     h->stats.columns = (long long)z.ncol;
     h->stats.systems = (long long)ns;

@@ -87,12 +87,14 @@ rt_fp64_kernel(const SegTable *__restrict__ st, const double *__restrict__ kv,
 
 // K1: stage the column and screen every system (optics sums, TLIMIT test,
 // DETAU, CUMTAUV); append kept systems to the family lists.
-__global__ void __launch_bounds__(224)
+template <bool F32>
+__global__ void __launch_bounds__(224, 2)
 rt_fp64_screen(const SegTable *__restrict__ st, int col_begin, int col_end, int max_nl,
                unsigned char *__restrict__ blocks, size_t stride, const double *__restrict__ kv,
                const double *__restrict__ ki, const double *__restrict__ planck, const RtConst K,
                int *__restrict__ list_v, int *__restrict__ list_i, unsigned int *counts,
-               uint32_t *status, unsigned long long *nsys) {
+               uint32_t *status, unsigned long long *nsys, const float *__restrict__ kvf,
+               const float *__restrict__ kif) {
     __shared__ int warp_v[8], warp_i[8], base_v, base_i;
     SysLocal w;
     unsigned int nsolved = 0;
@@ -108,14 +110,14 @@ rt_fp64_screen(const SegTable *__restrict__ st, int col_begin, int col_end, int 
         bool act_v = false, act_i = false;
         if (t < NSYS_V) {
             if (day) {
-                solve_vis<1>(sg, c, t / D_NG + 1, t % D_NG + 1, t, s, K, kv, w, nsolved, nullptr,
-                             nullptr, nullptr, nullptr, nullptr);
+                solve_vis<1, F32>(sg, c, t / D_NG + 1, t % D_NG + 1, t, s, K, kv, w, nsolved, nullptr,
+                                  nullptr, nullptr, nullptr, nullptr, kvf);
                 act_v = s.skip[t] == 0;
             }
         } else if (t < NSYS) {
             const int j = t - NSYS_V;
-            solve_ir<1>(sg, c, j / D_NG + 1, j % D_NG + 1, t, s, K, ki, w, nsolved, nullptr, nullptr,
-                        nullptr);
+            solve_ir<1, F32>(sg, c, j / D_NG + 1, j % D_NG + 1, t, s, K, ki, w, nsolved, nullptr, nullptr,
+                             nullptr, kif);
             act_i = s.skip[t] == 0;
         }
         const unsigned bv = __ballot_sync(0xffffffffu, act_v), bi = __ballot_sync(0xffffffffu, act_i);
@@ -152,6 +154,19 @@ rt_fp64_screen(const SegTable *__restrict__ st, int col_begin, int col_end, int 
         if (lane == 0 && v) atomicAdd(nsys, (unsigned long long)v);
     }
 }
+
+template __global__ void rt_fp64_screen<false>(const SegTable *__restrict__, int, int, int,
+                                               unsigned char *__restrict__, size_t, const double *__restrict__,
+                                               const double *__restrict__, const double *__restrict__,
+                                               const RtConst, int *__restrict__, int *__restrict__,
+                                               unsigned int *, uint32_t *, unsigned long long *,
+                                               const float *__restrict__, const float *__restrict__);
+template __global__ void rt_fp64_screen<true>(const SegTable *__restrict__, int, int, int,
+                                              unsigned char *__restrict__, size_t, const double *__restrict__,
+                                              const double *__restrict__, const double *__restrict__,
+                                              const RtConst, int *__restrict__, int *__restrict__,
+                                              unsigned int *, uint32_t *, unsigned long long *,
+                                              const float *__restrict__, const float *__restrict__);
 
 // K2: solve the listed systems of one family, one thread per system.
 template <bool VIS>

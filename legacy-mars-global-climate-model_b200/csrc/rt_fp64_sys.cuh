@@ -89,22 +89,43 @@ __device__ __forceinline__ double taugas_at(const ColSmem &s, int k, const doubl
     return s.u[k] * ans;
 }
 
+
+// TAUGAS at level k from the FP32 table of Cmk*k (mixed precision).
+__device__ __forceinline__ float taugas_f(const ColSmem &s, int k, const float *__restrict__ tb) {
+    const int mt = s.mt[k] - 1, mp = s.mp[k] - 1, nh = s.nh[k] - 1;
+    const int nh1 = nh + 1 < D_NH ? nh + 1 : D_NH - 1;
+    const float wr = (float)s.wr[k];
+    auto corner = [&](int a, int b) {
+        const float *p = tb + ((size_t)(a * D_NP + b) * D_NH) * D_NGK;
+        const float c0 = __ldg(p + nh * D_NGK), c1 = __ldg(p + nh1 * D_NGK);
+        return c0 + wr * (c1 - c0);
+    };
+    const float k1 = corner(mt, mp), k2 = corner(mt, mp + 1);
+    const float k3 = corner(mt + 1, mp + 1), k4 = corner(mt + 1, mp);
+    const float ans = (float)s.lk[4 * k] * k1 + (float)s.lk[4 * k + 1] * k2 +
+                      (float)s.lk[4 * k + 2] * k3 + (float)s.lk[4 * k + 3] * k4;
+    return (float)s.dpr[k] * ans;
+}
+
 // ---------------------------------------------------------------- visible
 // MODE 0: whole system (fused kernel); 1: screen only (optics, TLIMIT
 // decision, DETAU and CUMTAUV); 2: solve a system the screen kept.
-template <int MODE>
+// F32: opacities from the FP32 table of Cmk*k (mixed precision); everything
+// after the per-level optical depth stays FP64.
+template <int MODE, bool F32 = false>
 __device__ void solve_vis(const SegDev &sg, int c, int nw, int ng, int sidx, ColSmem &s,
                           const RtConst &K, const double *__restrict__ kv, SysLocal &w,
                           unsigned int &nsolved, double *fmp, double *fmm, double *sc0,
-                          double *sc1, double *sc2) {
+                          double *sc1, double *sc2, const float *__restrict__ kvf = nullptr) {
     const int L = sg.L, NL = L + 1;
     const double fz0 = K.fzerov[nw - 1];
     const bool band_skip = ng < D_NG && fz0 >= R4(0.99);
     const double *tb = kv + (size_t)(nw - 1) * D_NT * D_NP * D_NH * D_NGK + (ng - 1);
+    const float *tbf = F32 ? kvf + (size_t)(nw - 1) * D_NT * D_NP * D_NH * D_NGK + (ng - 1) : nullptr;
     double taugsurf = 0.0;
     auto dtauk = [&](int k) -> double {
         if (ng < D_NG) {
-            const double tg = taugas_at(s, k, tb);
+            const double tg = F32 ? (double)taugas_f(s, k, tbf) : taugas_at(s, k, tb);
             taugsurf += tg;
             return tg + s.trayaer[k * D_NV + nw - 1];
         }
@@ -260,10 +281,11 @@ __device__ void solve_vis(const SegDev &sg, int c, int nw, int ng, int sidx, Col
 }
 
 // ---------------------------------------------------------------- infrared
-template <int MODE>
+template <int MODE, bool F32 = false>
 __device__ void solve_ir(const SegDev &sg, int c, int nw, int ng, int sidx, ColSmem &s,
                          const RtConst &K, const double *__restrict__ ki, SysLocal &w,
-                         unsigned int &nsolved, double *fmp, double *fmm, double *sc0) {
+                         unsigned int &nsolved, double *fmp, double *fmm, double *sc0,
+                         const float *__restrict__ kif = nullptr) {
     const int L = sg.L, NL = L + 1, LEV = 2 * L + 3;
     const double fz0 = K.fzeroi[nw - 1];
     if (ng < D_NG && fz0 >= R4(0.99)) {
@@ -271,11 +293,12 @@ __device__ void solve_ir(const SegDev &sg, int c, int nw, int ng, int sidx, ColS
         return;
     }
     const double *tb = ki + (size_t)(nw - 1) * D_NT * D_NP * D_NH * D_NGK + (ng - 1);
+    const float *tbf = F32 ? kif + (size_t)(nw - 1) * D_NT * D_NP * D_NH * D_NGK + (ng - 1) : nullptr;
     double taugsurf = 0.0;
     auto dtauk = [&](int k) -> double {
         const double ta = s.taer_i[k * D_NI + nw - 1], tcl = s.tcld_i[k * D_NI + nw - 1];
         if (ng < D_NG) {
-            const double tg = taugas_at(s, k, tb);
+            const double tg = F32 ? (double)taugas_f(s, k, tbf) : taugas_at(s, k, tb);
             taugsurf += tg;
             return tg + ta + tcl;
         }
@@ -390,7 +413,7 @@ __device__ void solve_ir(const SegDev &sg, int c, int nw, int ng, int sidx, ColS
 
 // Ordered sums over (band, Gauss) of one output (code/sfluxv.f90:60-164,
 // code/sfluxi.f90:57-145).  q: 0 net, 1 up, 2 down (layer l), 3 top net, 4 DIFFV.
-__device__ double reduce_family(const ColSmem &s, const RtConst &K, bool vis, int q, int l,
+__device__ inline double reduce_family(const ColSmem &s, const RtConst &K, bool vis, int q, int l,
                                 int NL) {
     const int nb = vis ? D_NV : D_NI, base = vis ? 0 : NSYS_V;
     const double *fz = vis ? K.fzerov : K.fzeroi;
@@ -432,7 +455,7 @@ __device__ double reduce_family(const ColSmem &s, const RtConst &K, bool vis, in
 // Gauss point 17; IR ((val*DWNI)*GWEIGHT)*(1-FZEROI) or (val*DWNI)*FZERO
 // (code/sfluxv.f90:102-162, code/sfluxi.f90:95-143).  Unused factors are
 // exactly 1.0, which leaves the product bit-identical.  Returns the rows.
-__device__ int family_multipliers(const unsigned char *skip, const RtConst &K, bool vis,
+__device__ inline int family_multipliers(const unsigned char *skip, const RtConst &K, bool vis,
                                   double *m1, double *m2, double *m3) {
     const int nb = vis ? D_NV : D_NI, base = vis ? 0 : NSYS_V;
     const double *fz = vis ? K.fzerov : K.fzeroi;

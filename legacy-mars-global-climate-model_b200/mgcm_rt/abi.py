@@ -155,6 +155,7 @@ class Radiation:
             raise RTError(st.value, "mgcm_rt_create")
         self.precision = precision
         self.device = device
+        self._inflight: dict = {}
 
     def close(self):
         if getattr(self, "_h", None):
@@ -242,6 +243,41 @@ class Radiation:
             o["detau"] = b["detau"]
             o["cumtauv"] = b["cumtauv"]
         return outs
+
+    # ---- serving -------------------------------------------------------
+    def submit(self, b: dict, out: dict | None = None) -> tuple[int, dict]:
+        """Queue batch ``b``; returns (ticket, out).  Arrays must stay alive and
+        unmodified until ``wait`` returns; host DETAU/CUMTAUV are updated in
+        place."""
+        dev = _is_torch(b["plev"]) and b["plev"].is_cuda
+        keep: list = []
+        bi = make_in(b, dev, keep)
+        if out is None:
+            out = alloc_outputs(int(b["ncol"]), int(b["L"]),
+                                device=b["plev"].device if dev else None)
+        bo = make_out(out)
+        t = C.c_longlong(0)
+        rc = lib().mgcm_rt_submit(self._h, C.byref(bi), C.byref(bo), C.byref(t))
+        if rc != 0:
+            raise RTError(rc, "mgcm_rt_submit")
+        self._inflight[t.value] = (keep, bi, bo, b, out)
+        out["detau"], out["cumtauv"] = b["detau"], b["cumtauv"]
+        return t.value, out
+
+    def poll(self, ticket: int) -> int:
+        """1 finished, 0 pending; raises on an error status."""
+        rc = lib().mgcm_rt_poll(self._h, ticket)
+        if rc < 0:
+            raise RTError(rc, "mgcm_rt_poll")
+        return rc
+
+    def wait(self, ticket: int, timeout_s: float = -1.0) -> None:
+        rc = lib().mgcm_rt_wait(self._h, ticket, float(timeout_s))
+        if rc == -8:
+            raise RTError(rc, "mgcm_rt_wait")
+        self._inflight.pop(ticket, None)
+        if rc != 0:
+            raise RTError(rc, "mgcm_rt_wait")
 
     def dsolflux(self, sol, acosz, detau, dndiffv):
         dev = _is_torch(acosz)

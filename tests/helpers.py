@@ -63,3 +63,26 @@ def to_numpy(o):
     for k, v in o.items():
         out[k] = v.detach().cpu().numpy() if hasattr(v, "detach") else np.asarray(v)
     return out
+
+
+def mixed_errors(b, got, ref):
+    """Accuracy summary of a mixed-precision run against FP64:
+    max relative flux error (floor 1e-3 of the column flux scale) and the
+    heating-rate error in K/sol, both as dT/dt = QRAD*OM (temperature) and
+    as QRAD itself (potential temperature)."""
+    got = to_numpy(got)
+    fs = flux_scale(ref)[:, None]
+    out = {}
+    for k in FLUX_LAY:
+        d = np.abs(got[k] - ref[k]) / (np.abs(ref[k]) + 1e-3 * fs)
+        out[k] = float(d.max()) if d.size else 0.0
+    out["flux_max"] = max(out[k] for k in FLUX_LAY)
+    plev = np.asarray(b["plev"])
+    L = int(b["L"])
+    lev = 2 * L + 3
+    om = np.stack([(plev[:, 2 * l - 1] / plev[:, lev - 1]) ** KAPA for l in range(1, L + 2)], 1)
+    dth = np.abs(got["qrad"] - ref["qrad"]) * 88775.0
+    out["heat_dT_Ksol_max"] = float((dth * om).max()) if dth.size else 0.0
+    out["heat_dT_Ksol_rms"] = float(np.sqrt(((dth * om) ** 2).mean())) if dth.size else 0.0
+    out["heat_dtheta_Ksol_max"] = float(dth.max()) if dth.size else 0.0
+    return out
