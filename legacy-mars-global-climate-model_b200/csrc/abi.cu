@@ -34,13 +34,15 @@ __global__ void rt_fp64_kernel(const SegTable *__restrict__ st, const double *__
                                const double *__restrict__ ki, const double *__restrict__ planck,
                                const RtConst K, int max_nl, uint32_t *status,
                                unsigned long long *nsys, double *red_scratch);
+__global__ void rt_stage(const SegTable *__restrict__ st, int col_begin, int col_end, int max_nl,
+                         unsigned char *__restrict__ blocks, size_t stride,
+                         const double *__restrict__ planck, const RtConst K, uint32_t *status);
 template <bool F32>
 __global__ void rt_fp64_screen(const SegTable *__restrict__ st, int col_begin, int col_end, int max_nl,
                                unsigned char *__restrict__ blocks, size_t stride,
                                const double *__restrict__ kv, const double *__restrict__ ki,
-                               const double *__restrict__ planck, const RtConst K,
-                               int *__restrict__ list_v, int *__restrict__ list_i,
-                               unsigned int *counts, uint32_t *status, unsigned long long *nsys,
+                               const RtConst K, int *__restrict__ list_v, int *__restrict__ list_i,
+                               unsigned int *counts, unsigned long long *nsys,
                                const float *__restrict__ kvf, const float *__restrict__ kif);
 template <bool VIS>
 __global__ void rt_fp64_solve(const SegTable *__restrict__ st, int col_begin, int max_nl,
@@ -59,8 +61,11 @@ __global__ void rt_fp64_reduce(const SegTable *__restrict__ st, int col_begin, i
                                int max_nl, unsigned char *__restrict__ blocks, size_t stride,
                                const RtConst K, const double *__restrict__ fl_v,
                                const double *__restrict__ sc_v, const double *__restrict__ fl_i,
-                               const double *__restrict__ sc_i, uint32_t *status, int pool_rows);
-size_t reduce_smem_bytes(int max_nl, int rows);
+                               const double *__restrict__ sc_i, uint32_t *status, int rb);
+size_t reduce_smem_bytes(int max_nl, int rb);
+constexpr int REDUCE_WARPS = 4, REDUCE_THREADS = 32 * REDUCE_WARPS;   // rt_fp64_reduce: warp per column
+constexpr int STAGE_THREADS = 256, SCREEN_THREADS = 128;
+int reduce_rows_per_chunk(int max_nl);
 __global__ void rt_dsolflux_kernel(int ncol, const double *__restrict__ sol,
                                    const double *__restrict__ acosz,
                                    const double *__restrict__ detau,
@@ -156,7 +161,7 @@ struct Slot {
     uint32_t *d_status = nullptr, *h_status = nullptr;
     unsigned long long *d_nsys = nullptr, *h_nsys = nullptr;
     Arena stage, pipe, red;
-    int occ_nl = 0, occ_screen = 1, occ_solve = 1, occ_reduce = 1;
+    int occ_nl = 0, occ_stage = 1, occ_screen = 1, occ_solve = 1, occ_reduce = 1;
     bool busy = false;
     Job job;
     int kernels = 0;
@@ -412,17 +417,20 @@ int launch_pipeline(mgcm_rt_handle *h, Slot &sl, cudaStream_t st, int total, int
     double *sc_v = reinterpret_cast<double *>(take(n_v * 32));
     double *sc_i = reinterpret_cast<double *>(take(n_i * 32));
     unsigned int *counts = reinterpret_cast<unsigned int *>(take(256));
-    int pool_rows = (int)std::min<size_t>(NSYS, (48 * 1024) / (16 * (size_t)max_nl + 32));
-    if (pool_rows < 24) pool_rows = 0;
-    const size_t rsm = reduce_smem_bytes(max_nl, pool_rows);
+    const int rb = reduce_rows_per_chunk(max_nl);
+    const size_t rsm = reduce_smem_bytes(max_nl, rb);
     const bool mixed = h->cfg.precision == MGCM_RT_MIXED;
     if (sl.occ_nl != max_nl) {
         sl.occ_nl = max_nl;
         int a = 1, b = 1, c = 1;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, rt_fp64_screen<false>, BLOCK, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, mixed ? rt_fp64_screen<true> : rt_fp64_screen<false>,
+                                                      SCREEN_THREADS, 0);
+        int e = 1;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&e, rt_stage, STAGE_THREADS, 0);
+        sl.occ_stage = std::max(e, 1);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, rt_fp64_solve<false>, 128, 0);
         cudaFuncSetAttribute(rt_fp64_reduce, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rsm);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, rt_fp64_reduce, 160, rsm);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, rt_fp64_reduce, REDUCE_THREADS, rsm);
         sl.occ_screen = std::max(a, 1);
         sl.occ_solve = std::max(b, 1);
         if (const char *e = std::getenv("MGCM_RT_SOLVE_CTAS_PER_SM")) sl.occ_solve = std::max(1, std::atoi(e));
@@ -431,17 +439,20 @@ int launch_pipeline(mgcm_rt_handle *h, Slot &sl, cudaStream_t st, int total, int
     for (int c0 = 0; c0 < total; c0 += chunk) {
         const int c1 = std::min(total, c0 + chunk);
         CK(cudaMemsetAsync(counts, 0, 2 * sizeof(unsigned int), st));
-        const int g1 = std::min(c1 - c0, h->num_sms * sl.occ_screen);
+        const int g0 = std::min(c1 - c0, h->num_sms * sl.occ_stage);
+        rt_stage<<<g0, STAGE_THREADS, 0, st>>>(sl.d_segs, c0, c1, max_nl, blocks, stride, h->d_planck, h->K,
+                                               sl.d_status);
+        const long long items = (long long)(c1 - c0) * SCREEN_GROUPS;
+        const int warps = SCREEN_THREADS / 32;
+        const int g1 = (int)std::min<long long>((items + warps - 1) / warps, (long long)h->num_sms * sl.occ_screen);
         if (mixed)
-            rt_fp64_screen<true><<<g1, BLOCK, 0, st>>>(sl.d_segs, c0, c1, max_nl, blocks, stride,
-                                                       h->d_kv, h->d_ki, h->d_planck, h->K, list_v,
-                                                       list_i, counts, sl.d_status, sl.d_nsys,
-                                                       h->d_kvf, h->d_kif);
+            rt_fp64_screen<true><<<g1, SCREEN_THREADS, 0, st>>>(sl.d_segs, c0, c1, max_nl, blocks, stride,
+                                                                h->d_kv, h->d_ki, h->K, list_v, list_i,
+                                                                counts, sl.d_nsys, h->d_kvf, h->d_kif);
         else
-            rt_fp64_screen<false><<<g1, BLOCK, 0, st>>>(sl.d_segs, c0, c1, max_nl, blocks, stride,
-                                                        h->d_kv, h->d_ki, h->d_planck, h->K, list_v,
-                                                        list_i, counts, sl.d_status, sl.d_nsys,
-                                                        nullptr, nullptr);
+            rt_fp64_screen<false><<<g1, SCREEN_THREADS, 0, st>>>(sl.d_segs, c0, c1, max_nl, blocks, stride,
+                                                                 h->d_kv, h->d_ki, h->K, list_v, list_i,
+                                                                 counts, sl.d_nsys, nullptr, nullptr);
         const int g2 = h->num_sms * sl.occ_solve;
         if (mixed) {
             rt_mixed_solve<true><<<g2, 128, 0, st>>>(sl.d_segs, c0, max_nl, blocks, stride, h->d_kvf,
@@ -454,10 +465,10 @@ int launch_pipeline(mgcm_rt_handle *h, Slot &sl, cudaStream_t st, int total, int
             rt_fp64_solve<false><<<g2, 128, 0, st>>>(sl.d_segs, c0, max_nl, blocks, stride, h->d_ki,
                                                      h->K, list_i, counts, fl_i, sc_i);
         }
-        const int g3 = std::min(c1 - c0, h->num_sms * sl.occ_reduce);
-        rt_fp64_reduce<<<g3, 160, rsm, st>>>(sl.d_segs, c0, c1, max_nl, blocks, stride, h->K, fl_v,
-                                             sc_v, fl_i, sc_i, sl.d_status, pool_rows);
-        nk += 4;
+        const int g3 = std::min((c1 - c0 + REDUCE_WARPS - 1) / REDUCE_WARPS, h->num_sms * sl.occ_reduce);
+        rt_fp64_reduce<<<g3, REDUCE_THREADS, rsm, st>>>(sl.d_segs, c0, c1, max_nl, blocks, stride, h->K,
+                                                        fl_v, sc_v, fl_i, sc_i, sl.d_status, rb);
+        nk += 5;
         CK(cudaGetLastError());
     }
     return MGCM_RT_OK;

@@ -35,7 +35,7 @@ struct ColSmem {
     double *fmp, *fmm;                  // [sys][l]
     double *sc0, *sc1, *sc2;            // [sys] FLUXUP, FLUXDN, DIFFV (vis) / FTOPUP (IR)
     unsigned char *skip;                // [sys] 0 = solved, 1 = TLIMIT skip, 2 = no work
-    int *meta;                          // [4] list base/count of kept systems: vis, IR
+    int *meta;                          // [2*SCREEN_GROUPS] list base/count of kept systems per group
     double *fmnet_v, *fmnet_i;          // [l] reduced net fluxes for the divergences
     double *misc;                       // [4] NFLUXTOPV, NFLUXTOPI
     int day;
@@ -60,7 +60,7 @@ __host__ __device__ inline size_t col_smem_bytes(int nl, bool red_in_smem = true
     if (red_in_smem) b += red_bytes(nl);
     b += 3 * NSYS * sizeof(double);
     b += 2 * (nl + 1) * sizeof(double) + 4 * sizeof(double);
-    b += NSYS + 64;
+    b += NSYS + 16 + 2 * SCREEN_GROUPS * sizeof(int) + 16;
     return b;
 }
 

@@ -14,6 +14,19 @@ constexpr int NSYS_I = D_NI * D_NG;        // 85 IR systems per column
 constexpr int NSYS = NSYS_V + NSYS_I;      // 204
 constexpr int NREFV_IDX = 5;               // L_NREFV = 6 (0.67 um band), 0-based
 
+// Screening groups of a column: warp-sized runs of systems that never mix the
+// families -- visible 0-31, 32-63, 64-95, 96-118; IR 119-150, 151-182, 183-203.
+constexpr int SCREEN_GROUPS = 7, SCREEN_GROUPS_V = 4;
+__host__ __device__ constexpr int group_first(int w) {
+    return w < SCREEN_GROUPS_V ? 32 * w : NSYS_V + 32 * (w - SCREEN_GROUPS_V);
+}
+__host__ __device__ constexpr int group_end(int w) {
+    return w < SCREEN_GROUPS_V ? (32 * (w + 1) < NSYS_V ? 32 * (w + 1) : NSYS_V)
+                               : (NSYS_V + 32 * (w - SCREEN_GROUPS_V + 1) < NSYS
+                                      ? NSYS_V + 32 * (w - SCREEN_GROUPS_V + 1)
+                                      : NSYS);
+}
+
 // device status bits (OR-ed into the status word)
 constexpr uint32_t ST_PLANCK_RANGE = 1u;   // a Planck index left 1..8501 (clamped)
 constexpr uint32_t ST_NONFINITE = 2u;      // validation: NaN/Inf or p <= 0 in an input

@@ -85,68 +85,67 @@ rt_fp64_kernel(const SegTable *__restrict__ st, const double *__restrict__ kv,
 // per-system midpoint fluxes.  Solved systems are listed per family so the
 // solver keeps every thread busy (night columns and TLIMIT skips drop out).
 
-// K1: stage the column and screen every system (optics sums, TLIMIT test,
-// DETAU, CUMTAUV); append kept systems to the family lists.
+// K0: stage every column (bins, per-band opacity terms, Planck terms) into
+// its global block; one CTA per column.
+__global__ void __launch_bounds__(256)
+rt_stage(const SegTable *__restrict__ st, int col_begin, int col_end, int max_nl,
+         unsigned char *__restrict__ blocks, size_t stride, const double *__restrict__ planck,
+         const RtConst K, uint32_t *status) {
+    for (int g = col_begin + blockIdx.x; g < col_end; g += gridDim.x) {
+        const SegDev &sg = st->seg[find_seg(st, g)];
+        ColSmem s = carve_smem(blocks + (size_t)(g - col_begin) * stride, max_nl, nullptr, false);
+        stage_column(sg, g - sg.col0, K, planck, s, status);
+        __syncthreads();
+    }
+}
+
+// K1: screen every system (optics sums, TLIMIT test, DETAU, CUMTAUV) and
+// append the kept ones to the family lists.  One warp per (column, group);
+// warps never wait on one another.  A group's kept systems take one
+// contiguous run of list positions in ascending order; its base and count go
+// to the column's meta words.
 template <bool F32>
-__global__ void __launch_bounds__(224, 2)
+__global__ void __launch_bounds__(128)
 rt_fp64_screen(const SegTable *__restrict__ st, int col_begin, int col_end, int max_nl,
                unsigned char *__restrict__ blocks, size_t stride, const double *__restrict__ kv,
-               const double *__restrict__ ki, const double *__restrict__ planck, const RtConst K,
-               int *__restrict__ list_v, int *__restrict__ list_i, unsigned int *counts,
-               uint32_t *status, unsigned long long *nsys, const float *__restrict__ kvf,
-               const float *__restrict__ kif) {
-    __shared__ int warp_v[8], warp_i[8], base_v, base_i;
+               const double *__restrict__ ki, const RtConst K, int *__restrict__ list_v,
+               int *__restrict__ list_i, unsigned int *counts, unsigned long long *nsys,
+               const float *__restrict__ kvf, const float *__restrict__ kif) {
     SysLocal w;
     unsigned int nsolved = 0;
-    const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
-    for (int g = col_begin + blockIdx.x; g < col_end; g += gridDim.x) {
-        const int si = find_seg(st, g);
-        const SegDev &sg = st->seg[si];
+    const int lane = threadIdx.x & 31;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    const long long items = (long long)(col_end - col_begin) * SCREEN_GROUPS;
+    for (long long it = (long long)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); it < items; it += nwarps) {
+        const int g = col_begin + (int)(it / SCREEN_GROUPS), grp = (int)(it % SCREEN_GROUPS);
+        const SegDev &sg = st->seg[find_seg(st, g)];
         const int c = g - sg.col0;
         ColSmem s = carve_smem(blocks + (size_t)(g - col_begin) * stride, max_nl, nullptr, false);
-        const bool day = sg.acosz[c] >= R4(1.0e-5);
-        stage_column(sg, c, K, planck, s, status);
-        __syncthreads();
-        bool act_v = false, act_i = false;
-        if (t < NSYS_V) {
-            if (day) {
+        const bool vis = grp < SCREEN_GROUPS_V;
+        const int t = group_first(grp) + lane;
+        bool act = false;
+        if (vis) {
+            if (t < group_end(grp) && sg.acosz[c] >= R4(1.0e-5)) {
                 solve_vis<1, F32>(sg, c, t / D_NG + 1, t % D_NG + 1, t, s, K, kv, w, nsolved, nullptr,
                                   nullptr, nullptr, nullptr, nullptr, kvf);
-                act_v = s.skip[t] == 0;
+                act = s.skip[t] == 0;
             }
-        } else if (t < NSYS) {
+        } else if (t < group_end(grp)) {
             const int j = t - NSYS_V;
             solve_ir<1, F32>(sg, c, j / D_NG + 1, j % D_NG + 1, t, s, K, ki, w, nsolved, nullptr, nullptr,
                              nullptr, kif);
-            act_i = s.skip[t] == 0;
+            act = s.skip[t] == 0;
         }
-        const unsigned bv = __ballot_sync(0xffffffffu, act_v), bi = __ballot_sync(0xffffffffu, act_i);
+        const unsigned m = __ballot_sync(0xffffffffu, act);
+        const int n = __popc(m);
+        int base = 0;
         if (lane == 0) {
-            warp_v[wid] = __popc(bv);
-            warp_i[wid] = __popc(bi);
+            base = n ? (int)atomicAdd(&counts[vis ? 0 : 1], (unsigned)n) : 0;
+            s.meta[2 * grp] = base;
+            s.meta[2 * grp + 1] = n;
         }
-        __syncthreads();
-        if (t == 0) {
-            int nv = 0, ni = 0;
-            for (int q = 0; q < (int)(blockDim.x >> 5); ++q) {
-                const int a = warp_v[q], b = warp_i[q];
-                warp_v[q] = nv;
-                warp_i[q] = ni;
-                nv += a;
-                ni += b;
-            }
-            base_v = nv ? (int)atomicAdd(&counts[0], (unsigned)nv) : 0;
-            base_i = ni ? (int)atomicAdd(&counts[1], (unsigned)ni) : 0;
-            s.meta[0] = base_v;
-            s.meta[1] = nv;
-            s.meta[2] = base_i;
-            s.meta[3] = ni;
-        }
-        __syncthreads();
-        const unsigned below = (1u << lane) - 1u;
-        if (act_v) list_v[base_v + warp_v[wid] + __popc(bv & below)] = (g << 8) | t;
-        if (act_i) list_i[base_i + warp_i[wid] + __popc(bi & below)] = (g << 8) | t;
-        __syncthreads();
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (act) (vis ? list_v : list_i)[base + __popc(m & ((1u << lane) - 1u))] = (g << 8) | t;
     }
     if (nsys) {
         unsigned int v = nsolved;
@@ -155,18 +154,14 @@ rt_fp64_screen(const SegTable *__restrict__ st, int col_begin, int col_end, int 
     }
 }
 
-template __global__ void rt_fp64_screen<false>(const SegTable *__restrict__, int, int, int,
-                                               unsigned char *__restrict__, size_t, const double *__restrict__,
-                                               const double *__restrict__, const double *__restrict__,
-                                               const RtConst, int *__restrict__, int *__restrict__,
-                                               unsigned int *, uint32_t *, unsigned long long *,
-                                               const float *__restrict__, const float *__restrict__);
-template __global__ void rt_fp64_screen<true>(const SegTable *__restrict__, int, int, int,
-                                              unsigned char *__restrict__, size_t, const double *__restrict__,
-                                              const double *__restrict__, const double *__restrict__,
-                                              const RtConst, int *__restrict__, int *__restrict__,
-                                              unsigned int *, uint32_t *, unsigned long long *,
-                                              const float *__restrict__, const float *__restrict__);
+#define SCREEN_ARGS                                                                                    \
+    const SegTable *__restrict__, int, int, int, unsigned char *__restrict__, size_t,                \
+        const double *__restrict__, const double *__restrict__, const RtConst, int *__restrict__,    \
+        int *__restrict__, unsigned int *, unsigned long long *, const float *__restrict__,          \
+        const float *__restrict__
+template __global__ void rt_fp64_screen<false>(SCREEN_ARGS);
+template __global__ void rt_fp64_screen<true>(SCREEN_ARGS);
+#undef SCREEN_ARGS
 
 // K2: solve the listed systems of one family, one thread per system.
 template <bool VIS>
@@ -206,95 +201,277 @@ template __global__ void rt_fp64_solve<false>(const SegTable *__restrict__, int,
                                               const int *__restrict__, const unsigned int *,
                                               double *__restrict__, double *__restrict__);
 
-// K3: ordered sums and heating per column.  The column's kept systems sit
-// in contiguous rows of the compact flux buffers; one thread pulls them into
-// shared memory with TMA bulk copies completed on an mbarrier, then one
-// thread per output sums them in the reference order.
-__global__ void __launch_bounds__(160)
+// K3: ordered sums and heating, one warp per column.  A column's kept systems
+// sit in contiguous rows of the compact flux buffers (visible, then IR).  Lane
+// 0 streams them in chunks of `rb` rows through a ring of RED_STAGES shared
+// buffers with TMA bulk copies completed on mbarriers (next chunks in flight
+// while the current one is summed); lane j owns levels j+1, j+33, ... and sums
+// its outputs over the rows in the reference order (rows are in ascending
+// (band, Gauss) order, each scaled by the multipliers of family_multipliers).
+constexpr int RED_WARPS = 4;
+constexpr int RED_STAGES = 4;
+constexpr int RED_LPL = (D_MAXNL + 1 + 31) / 32;   // levels per lane
+
+__host__ __device__ inline size_t red_warp_bytes(int max_nl, int rb) {
+    const size_t rowb = (size_t)16 * max_nl + 32;
+    size_t b = (size_t)RED_STAGES * rb * rowb;        // ring
+    b += (size_t)3 * NSYS * 8;                        // multipliers
+    b += (size_t)2 * (D_MAXNL + 2) * 8 + 4 * 8;       // FMNET per level, top values
+    b += (size_t)RED_STAGES * 8;                      // mbarriers
+    return (b + 127) / 128 * 128;
+}
+
+// Multipliers of both families for one column, one lane per band (visible
+// bands on lanes 0-6, IR bands on lanes 8-12); each lane walks its band as
+// family_multipliers does, at the band's offset among the kept rows.
+__device__ inline void warp_multipliers(const unsigned char *skip, bool day, const RtConst &K,
+                                        double *m1, double *m2, double *m3) {
+    const int lane = threadIdx.x & 31;
+    const bool isv = lane < D_NV && day, isi = lane >= 8 && lane < 8 + D_NI;
+    const int nw = isv ? lane + 1 : (isi ? lane - 7 : 0);
+    const int base = isv ? 0 : NSYS_V;
+    const double fz = isv ? K.fzerov[nw - 1] : (isi ? K.fzeroi[nw - 1] : 0.0);
+    const unsigned char *sk = skip + base + (nw > 0 ? nw - 1 : 0) * D_NG;
+    int cnt = 0;
+    if (isv || isi) {
+        if (!(fz >= R4(0.99)))
+            for (int ng = 1; ng <= D_NG - 1; ++ng) cnt += sk[ng - 1] == 0;
+        cnt += 1;
+    }
+    // exclusive prefix over the lanes of the same family
+    const int first = isv ? 0 : 8;
+    int pos = 0;
+    for (int k = 1; k < 8; ++k) {
+        const int v = __shfl_up_sync(0xffffffffu, cnt, k);
+        if (lane - k >= first) pos += v;
+    }
+    if (!(isv || isi)) return;
+    double *p1 = m1 + base, *p2 = m2 + base, *p3 = m3 + base;
+    double fzero = fz;
+    const double dw = isv ? 1.0 : K.dwni[nw - 1];
+    if (!(fz >= R4(0.99))) {
+        for (int ng = 1; ng <= D_NG - 1; ++ng) {
+            if (sk[ng - 1] != 0) {
+                fzero = fzero + (1.0 - fz) * K.gweight[ng - 1];
+                continue;
+            }
+            if (isv) {
+                p1[pos] = K.gweight[ng - 1];
+                p2[pos] = 1.0 - fz;
+                p3[pos] = 1.0;
+            } else {
+                p1[pos] = dw;
+                p2[pos] = K.gweight[ng - 1];
+                p3[pos] = 1.0 - fz;
+            }
+            ++pos;
+        }
+    }
+    if (isv) {
+        p1[pos] = fzero;
+        p2[pos] = 1.0;
+    } else {
+        p1[pos] = dw;
+        p2[pos] = fzero;
+    }
+    p3[pos] = 1.0;
+}
+
+__global__ void __launch_bounds__(32 * RED_WARPS)
 rt_fp64_reduce(const SegTable *__restrict__ st, int col_begin, int col_end, int max_nl,
                unsigned char *__restrict__ blocks, size_t stride, const RtConst K,
                const double *__restrict__ fl_v, const double *__restrict__ sc_v,
                const double *__restrict__ fl_i, const double *__restrict__ sc_i,
-               uint32_t *status, int pool_rows) {
+               uint32_t *status, int rb) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    __shared__ __align__(8) uint64_t bar;
-    __shared__ unsigned char skip[NSYS];
-    __shared__ double fmnet_v[D_MAXNL + 1], fmnet_i[D_MAXNL + 1], misc[4];
-    __shared__ double mv[3][NSYS_V], mi[3][NSYS_I];
-    __shared__ int rows_v, rows_i;
-    const size_t row = (size_t)2 * max_nl;
-    // a pool of cap_rows rows (visible rows first, then IR) and their scalars
-    const int cap_rows = pool_rows;
-    double *pool = reinterpret_cast<double *>(smem_raw);
-    double *scpool = pool + (size_t)cap_rows * row;
-    const int t = threadIdx.x;
-    if (t == 0) mbar_init(&bar, 1);
-    __syncthreads();
-    uint32_t phase = 0;
-    for (int g = col_begin + blockIdx.x; g < col_end; g += gridDim.x) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const size_t row = (size_t)2 * max_nl;   // doubles per compact row
+    const uint32_t rowb = (uint32_t)(row * 8), chunkb = (uint32_t)rb * (rowb + 32);
+    unsigned char *ws = smem_raw + (size_t)wid * red_warp_bytes(max_nl, rb);
+    unsigned char *ring = ws;
+    double *m1 = reinterpret_cast<double *>(ws + (size_t)RED_STAGES * chunkb);
+    double *m2 = m1 + NSYS, *m3 = m2 + NSYS;
+    double *fmv = m3 + NSYS, *fmi = fmv + (D_MAXNL + 2), *misc = fmi + (D_MAXNL + 2);
+    uint64_t *bar = reinterpret_cast<uint64_t *>(misc + 4);
+    if (lane == 0)
+        for (int k = 0; k < RED_STAGES; ++k) mbar_init(&bar[k], 1);
+    __syncwarp();
+    unsigned int gf = 0, gc = 0;   // chunks issued / consumed by this warp
+
+    for (int g = col_begin + blockIdx.x * RED_WARPS + wid; g < col_end; g += gridDim.x * RED_WARPS) {
         const int si = find_seg(st, g);
         const SegDev &sg = st->seg[si];
         const int c = g - sg.col0;
+        const int NL = sg.L + 1;
         const ColSmem s = carve_smem(blocks + (size_t)(g - col_begin) * stride, max_nl, nullptr, false);
         const bool day = sg.acosz[c] >= R4(1.0e-5);
-        const int bv = s.meta[0], nv = day ? s.meta[1] : 0, bi = s.meta[2], ni = s.meta[3];
-        double *flv = pool, *fli = pool + (size_t)nv * row;
-        double *scv = scpool, *sci = scpool + (size_t)nv * 4;
-        if (nv + ni > cap_rows) {   // more kept systems than the pool holds: sum from global memory
-            for (int i = t; i < NSYS; i += blockDim.x) skip[i] = (i < NSYS_V && !day) ? 2 : s.skip[i];
-            __syncthreads();
-            if (t == 0 && day) rows_v = family_multipliers(skip, K, true, mv[0], mv[1], mv[2]);
-            if (t == 32) rows_i = family_multipliers(skip, K, false, mi[0], mi[1], mi[2]);
-            __syncthreads();
-            reduce_and_heat(
-                sg, c,
-                [&](bool vis, int q, int l) {
-                    return vis ? reduce_rows(fl_v + (size_t)bv * row, sc_v + (size_t)bv * 4, max_nl,
-                                             rows_v, mv[0], mv[1], mv[2], true, q, l)
-                               : reduce_rows(fl_i + (size_t)bi * row, sc_i + (size_t)bi * 4, max_nl,
-                                             rows_i, mi[0], mi[1], mi[2], false, q, l);
-                },
-                fmnet_v, fmnet_i, misc, day);
-            __syncthreads();
-            continue;
+        // kept rows per screening group (visible groups empty at night)
+        int gbase[SCREEN_GROUPS], gcnt[SCREEN_GROUPS], nch = 0;
+#pragma unroll
+        for (int w = 0; w < SCREEN_GROUPS; ++w) {
+            gbase[w] = s.meta[2 * w];
+            gcnt[w] = (w < SCREEN_GROUPS_V && !day) ? 0 : s.meta[2 * w + 1];
+            nch += (gcnt[w] + rb - 1) / rb;
         }
-        if (t == 0) {
-            fence_proxy_async_smem();
-            const uint32_t bytes = (uint32_t)((nv + ni) * (row * 8 + 32));
-            mbar_arrive_expect_tx(&bar, bytes);
-            if (nv) {
-                bulk_g2s(flv, fl_v + (size_t)bv * row, (uint32_t)(nv * row * 8), &bar);
-                bulk_g2s(scv, sc_v + (size_t)bv * 4, (uint32_t)(nv * 32), &bar);
+        // chunk j -> family, first list position, family row index, rows
+        auto chunk = [&](int j, bool &vis, int &b0, int &fr, int &cnt) {
+            int off = 0;
+#pragma unroll
+            for (int w = 0; w < SCREEN_GROUPS; ++w) {
+                if (w == SCREEN_GROUPS_V) off = 0;
+                const int nc = (gcnt[w] + rb - 1) / rb;
+                if (j >= 0 && j < nc) {
+                    vis = w < SCREEN_GROUPS_V;
+                    b0 = gbase[w] + j * rb;
+                    fr = off + j * rb;
+                    cnt = min(rb, gcnt[w] - j * rb);
+                }
+                j -= nc;
+                off += gcnt[w];
             }
-            if (ni) {
-                bulk_g2s(fli, fl_i + (size_t)bi * row, (uint32_t)(ni * row * 8), &bar);
-                bulk_g2s(sci, sc_i + (size_t)bi * 4, (uint32_t)(ni * 32), &bar);
+        };
+        auto issue = [&](int j) {
+            if (lane == 0) {
+                bool vis = true;
+                int b0 = 0, fr = 0, cnt = 0;
+                chunk(j, vis, b0, fr, cnt);
+                unsigned char *dst = ring + (size_t)(gf % RED_STAGES) * chunkb;
+                fence_proxy_async_smem();
+                mbar_arrive_expect_tx(&bar[gf % RED_STAGES], (uint32_t)cnt * (rowb + 32));
+                bulk_g2s(dst, (vis ? fl_v : fl_i) + (size_t)b0 * row, (uint32_t)cnt * rowb,
+                         &bar[gf % RED_STAGES]);
+                bulk_g2s(dst + (size_t)rb * rowb, (vis ? sc_v : sc_i) + (size_t)b0 * 4,
+                         (uint32_t)cnt * 32, &bar[gf % RED_STAGES]);
             }
+            ++gf;
+        };
+        int next = 0;
+        while (next < nch && gf - gc < RED_STAGES) issue(next++);
+        warp_multipliers(s.skip, day, K, m1, m2, m3);
+        __syncwarp();
+
+        double acc[3][RED_LPL], top = 0.0, dif = 0.0;
+        auto clear = [&]() {
+#pragma unroll
+            for (int q = 0; q < 3; ++q)
+#pragma unroll
+                for (int r = 0; r < RED_LPL; ++r) acc[q][r] = 0.0;
+            top = 0.0;
+            dif = 0.0;
+        };
+        // family outputs, FMNET kept for the heating
+        auto flush = [&](bool vis) {
+#pragma unroll
+            for (int r = 0; r < RED_LPL; ++r) {
+                const int l = lane + 1 + 32 * r;
+                if (l > NL) break;
+                const size_t o = (size_t)c * NL + l - 1;
+                if (vis) {
+                    sg.fmnetv[o] = acc[0][r];
+                    sg.fluxupv[o] = acc[1][r];
+                    sg.fluxdnv[o] = acc[2][r];
+                    fmv[l] = acc[0][r];
+                    if (l == NL) {
+                        sg.dnvflux[c] = acc[2][r];
+                        sg.fluxsurf[c] = (1.0 - sg.als[c]) * acc[2][r];
+                    }
+                } else {
+                    sg.fmneti[o] = acc[0][r];
+                    sg.fluxupi[o] = acc[1][r];
+                    sg.fluxdni[o] = acc[2][r];
+                    fmi[l] = acc[0][r];
+                    if (l == NL) sg.dnirflux[c] = acc[2][r];
+                }
+            }
+            if (lane == 0) {
+                if (vis) {
+                    sg.nfluxtopv[c] = top;
+                    sg.diffvt[c] = dif;
+                    sg.dndiffv[c] = dif;
+                    misc[0] = top;
+                } else {
+                    sg.nfluxtopi[c] = top;
+                    misc[1] = top;
+                }
+            }
+        };
+        clear();
+        bool cur_vis = true;
+        for (int j = 0; j < nch; ++j) {
+            bool vis = true;
+            int b0 = 0, r0 = 0, cnt = 0;
+            chunk(j, vis, b0, r0, cnt);
+            if (vis != cur_vis) {   // visible rows done
+                flush(true);
+                clear();
+                cur_vis = false;
+            }
+            const unsigned int stg = gc % RED_STAGES;
+            if (!mbar_wait(&bar[stg], (gc / RED_STAGES) & 1u, status)) {
+                for (++gc; gc < gf; ++gc) mbar_wait(&bar[gc % RED_STAGES], (gc / RED_STAGES) & 1u, status);
+                return;   // copies drained; status holds the error
+            }
+            const double *buf = reinterpret_cast<const double *>(ring + (size_t)stg * chunkb);
+            const double *scb = reinterpret_cast<const double *>(ring + (size_t)stg * chunkb + (size_t)rb * rowb);
+            const double *f1 = (vis ? m1 : m1 + NSYS_V) + r0, *f2 = (vis ? m2 : m2 + NSYS_V) + r0,
+                         *f3 = (vis ? m3 : m3 + NSYS_V) + r0;
+            for (int k = 0; k < cnt; ++k) {
+                const double a = f1[k], b = f2[k], e = f3[k];
+                const double *pr = buf + (size_t)k * row;
+#pragma unroll
+                for (int r = 0; r < RED_LPL; ++r) {
+                    const int l = lane + 1 + 32 * r;
+                    if (l > NL) break;
+                    const double up = pr[l - 1], dn = pr[max_nl + l - 1];
+                    acc[0][r] = acc[0][r] + (up - dn) * a * b * e;
+                    acc[1][r] = acc[1][r] + up * a * b * e;
+                    acc[2][r] = acc[2][r] + dn * a * b * e;
+                }
+                const double *sk = scb + (size_t)k * 4;
+                if (vis) {
+                    top = top + (sk[0] - sk[1]) * a * b * e;
+                    dif = dif + sk[2] * a * b * e;
+                } else {
+                    top = top + sk[0] * a * b * e;
+                }
+            }
+            ++gc;
+            __syncwarp();
+            if (next < nch) issue(next++);
         }
-        for (int i = t; i < NSYS; i += blockDim.x) skip[i] = (i < NSYS_V && !day) ? 2 : s.skip[i];
-        __syncthreads();
-        if (t == 0 && day) rows_v = family_multipliers(skip, K, true, mv[0], mv[1], mv[2]);
-        if (t == 32) rows_i = family_multipliers(skip, K, false, mi[0], mi[1], mi[2]);
-        const bool ok = mbar_wait(&bar, phase, status);
-        phase ^= 1u;
-        __syncthreads();
-        if (!ok) {   // copies still in flight: wait for them again, then give up
-            mbar_wait(&bar, phase ^ 1u, status);
-            return;
+        if (cur_vis) {   // no IR chunk followed: visible outputs (zeros at night)
+            flush(true);
+            clear();
         }
-        reduce_and_heat(
-            sg, c,
-            [&](bool vis, int q, int l) {
-                return vis ? reduce_rows(flv, scv, max_nl, rows_v, mv[0], mv[1], mv[2], true, q, l)
-                           : reduce_rows(fli, sci, max_nl, rows_i, mi[0], mi[1], mi[2], false, q, l);
-            },
-            fmnet_v, fmnet_i, misc, day);
-        __syncthreads();
+        flush(false);
+        __syncwarp();
+        // divergences and heating rates (code/comp3.f:677-681,735-738,765-771)
+        const double *plev = sg.plev + (size_t)c * (2 * sg.L + 3);
+        const int LEV = 2 * sg.L + 3;
+        for (int l = 1 + lane; l <= NL; l += 32) {
+            const double sun = day ? (l == 1 ? fmv[1] - misc[0] : fmv[l] - fmv[l - 1]) : 0.0;
+            const double irt = l == 1 ? fmi[1] - misc[1] : fmi[l] - fmi[l - 1];
+            const int k = 2 * l;
+            const double ptrop = sg.ptrop, p = sg.pcol[c];
+            const double ym = k == 2 ? ptrop * 100.0 / 3.72 : (plev[k + 1 - 1] - plev[k - 1 - 1]) * 100.0 / 3.72;
+            const double om = pow(plev[k - 1] / plev[LEV - 1], 0.25684);
+            const double pnlte = sg.sigma[k - 1] * (p - ptrop) + ptrop;
+            const double sunlte = sun * 2.2e4 * pnlte / (1.0 + 2.2e4 * pnlte);
+            const size_t o = (size_t)c * NL + l - 1;
+            sg.suntot[o] = sun;
+            sg.irtotal[o] = irt;
+            sg.qrad[o] = (sunlte + irt) / (735.94 * ym * om);
+        }
+        __syncwarp();
     }
 }
 
-// Shared memory of rt_fp64_reduce: a pool of `rows` kept-system rows.
-size_t reduce_smem_bytes(int max_nl, int rows) { return (size_t)rows * (16 * max_nl + 32); }
+// Shared memory of rt_fp64_reduce with `rb` rows per chunk.
+size_t reduce_smem_bytes(int max_nl, int rb) { return (size_t)RED_WARPS * red_warp_bytes(max_nl, rb); }
+int reduce_rows_per_chunk(int max_nl) {
+    const int rowb = 16 * max_nl + 32;
+    return std::max(1, std::min(8, 2048 / rowb));
+}
 
 // Partial radiation: DIRECTSOL from DETAU (code/dsolflux.f:28-45) and
 // DNVFLUX = DNDIFFV + DIRECTSOL (code/comp3.f:335-351).
