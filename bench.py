@@ -60,6 +60,18 @@ def algorithmic_bytes_per_column(L: int, cloud: bool) -> int:
     return 8 * (n_in + n_out + n_state)
 
 
+def traffic_per_step(precision: str, ncol: int):
+    """DRAM bytes (read + write) of one call's kernels from the committed ncu
+    summary (profiles/pipeline_traffic.json, an 8,192-column capture), scaled
+    to `ncol` columns; None when absent."""
+    try:
+        j = json.loads((ROOT / "profiles" / "pipeline_traffic.json").read_text())
+        e = j[precision]
+        return float(e["dram_bytes"]) * ncol / float(e["columns"])
+    except Exception:
+        return None
+
+
 def peaks():
     try:
         j = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
@@ -176,16 +188,137 @@ def run_reference(args, wl):
     print(json.dumps(line), flush=True)
 
 
+def time_device(rt, bd, out, steps, warmup, stream, barrier, clk=None):
+    """K steps of one radiation call on device-resident inputs; returns
+    (ms per step from CUDA events on the launching stream, per-call pipeline
+    ms from the library's own events, stats)."""
+    import torch
+    rt.set_stream(stream)
+    for _ in range(warmup):
+        rt.enqueue(bd, out)
+        rt.sync()
+    kern_ms = []
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        rt.enqueue(bd, out)
+        rt.sync()
+        kern_ms.append(rt.stats()["gpu_ms"])
+    e1.record(stream)
+    barrier()
+    return e0.elapsed_time(e1) / steps, kern_ms, rt.stats()
+
+
+def accuracy(bd, got, ref, L):
+    """Mixed vs FP64 on the whole batch: max relative flux error (floor 1e-3
+    of the column's flux scale) and heating-rate error in K/sol, as
+    dT/dt = QRAD*OM and as QRAD (potential temperature)."""
+    import torch
+    flux = ("fmnetv", "fluxupv", "fluxdnv", "fmneti", "fluxupi", "fluxdni")
+    fs = torch.stack([ref[k].abs().amax(dim=1) for k in flux], 1).amax(dim=1, keepdim=True)
+    fe = max(float(((got[k] - ref[k]).abs() / (ref[k].abs() + 1e-3 * fs)).max()) for k in flux)
+    lev = 2 * L + 3
+    plev = bd["plev"]
+    om = torch.stack([(plev[:, 2 * l - 1] / plev[:, lev - 1]) ** 0.25684 for l in range(1, L + 2)], 1)
+    dth = (got["qrad"] - ref["qrad"]).abs() * 88775.0
+    dT = dth * om
+    return {"flux_rel_max": fe, "heat_dT_Ksol_max": float(dT.max()),
+            "heat_dT_Ksol_rms": float(dT.pow(2).mean().sqrt()), "heat_dtheta_Ksol_max": float(dth.max()),
+            "tolerance": {"flux_rel": 1e-3, "heat_Ksol": 1e-2}, "against": "FP64 GPU path (= FP64 oracle to 1e-12)"}
+
+
+def serving(rt, device, seed, rate=200.0, duration_s=1.0, base_cols=200_000):
+    """Open-loop request stream through mgcm_rt_submit/poll: Poisson arrivals
+    at `rate`/s for `duration_s`, sizes log-uniform in [1k, 200k] columns,
+    L uniform in {24, 36, 48}; inputs device-resident (views into one tiled
+    synthetic batch per L).  Latency = completion - scheduled arrival.  Then
+    20 isolated 64k-column requests (L24, closed loop)."""
+    import torch
+    from mgcm_rt import abi, synth
+    rng = np.random.default_rng(seed)
+    bases = {}
+    for L in (24, 36, 48):
+        b = synth.make_batch(20_000, L=L, seed=seed + L, cloud=True)
+        rep = (base_cols + 19_999) // 20_000
+        bases[L] = {k: (torch.from_numpy(np.ascontiguousarray(v)).to(device).repeat(
+                        (rep,) + (1,) * (v.ndim - 1))[:base_cols].contiguous()
+                        if isinstance(v, np.ndarray) and k not in ("sigma", "sol") else
+                        (torch.from_numpy(np.ascontiguousarray(v)).to(device) if isinstance(v, np.ndarray) else v))
+                    for k, v in b.items()}
+        bases[L]["ncol"] = base_cols
+    def request(L, n):
+        off = int(rng.integers(0, base_cols - n + 1))
+        r = {k: (v[off:off + n] if torch.is_tensor(v) and k not in ("sigma", "sol") else v)
+             for k, v in bases[L].items()}
+        r["ncol"] = n
+        return r, abi.alloc_outputs(n, L, device=device)
+    # warm the serving slots
+    for L in (24, 36, 48):
+        r, o = request(L, 40_000)
+        t, _ = rt.submit(r, o)
+        rt.wait(t, 60.0)
+    gaps = rng.exponential(1.0 / rate, size=int(rate * duration_s * 3) + 10)
+    arr = np.cumsum(gaps)
+    arr = arr[arr < duration_s]
+    sizes = np.exp(rng.uniform(np.log(1000), np.log(200_000), size=len(arr))).astype(int)
+    Ls = rng.choice([24, 36, 48], size=len(arr))
+    reqs = [request(int(L), int(n)) for L, n in zip(Ls, sizes)]
+    torch.cuda.synchronize()
+    pending, lat = [], []
+    i = 0
+    t0 = time.perf_counter()
+    while i < len(arr) or pending:
+        now = time.perf_counter() - t0
+        while i < len(arr) and arr[i] <= now:
+            t, _ = rt.submit(*reqs[i])
+            pending.append((t, arr[i], int(sizes[i])))
+            i += 1
+        still = []
+        for p in pending:
+            if rt.poll(p[0]) == 1:
+                lat.append(((time.perf_counter() - t0 - p[1]) * 1e3, p[2]))
+                rt.wait(p[0], 0.0)
+            else:
+                still.append(p)
+        pending = still
+        time.sleep(5e-5)
+    t_end = time.perf_counter() - t0
+    ms = np.array([x[0] for x in lat])
+    cols = int(sizes.sum())
+    # isolated 64k-column requests
+    iso = []
+    r, o = request(24, 65_536)
+    for _ in range(23):
+        t1 = time.perf_counter()
+        t, _ = rt.submit(r, o)
+        rt.wait(t, 60.0)
+        iso.append((time.perf_counter() - t1) * 1e3)
+    iso = np.array(iso[3:])
+    offered = cols / duration_s
+    achieved = cols / t_end
+    return {"requests": int(len(arr)), "rate_per_s": rate, "duration_s": duration_s,
+            "sizes": "log-uniform [1k, 200k] columns, L in {24, 36, 48}, device-resident inputs",
+            "p50_ms": float(np.percentile(ms, 50)), "p99_ms": float(np.percentile(ms, 99)),
+            "offered_cols_per_s": offered, "achieved_cols_per_s": achieved,
+            "sustainable": bool(achieved >= 0.98 * offered),
+            "isolated_64k": {"p50_ms": float(np.percentile(iso, 50)), "p99_ms": float(np.percentile(iso, 99)),
+                             "reps": int(len(iso)), "layers": 24}}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="both", choices=["both", "fp64", "mixed"],
+                    help="both: the headline value is the mixed path, FP64 is timed beside it")
     ap.add_argument("--workload", default="c1", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-serving", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     wl = WORKLOADS[args.workload]
@@ -200,57 +333,54 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
     dist = None
     if world > 1:
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     d, kind = data.ensure_data()
-    prec = abi.MIXED if args.precision == "mixed" else abi.FP64
-    rt = abi.Radiation(d, max_layers=wl["L"], precision=prec, device=local, validate=False)
-    b = synth.make_batch(wl["ncol"], L=wl["L"], seed=1000 + rank, cloud=wl["cloud"])
-    ncol = wl["ncol"]
+    L, ncol = wl["L"], wl["ncol"]
+    b = synth.make_batch(ncol, L=L, seed=1000 + rank, cloud=wl["cloud"])
     stream = torch.cuda.Stream()
-    rt.set_stream(stream)
-
-    # ---- device-resident inputs (value)
-    bd = {k: (torch.from_numpy(np.ascontiguousarray(v)).cuda() if isinstance(v, np.ndarray) else v)
-          for k, v in b.items()}
-    out = abi.alloc_outputs(ncol, wl["L"], device=torch.device("cuda", local))
-    for _ in range(args.warmup):
-        rt.enqueue(bd, out)
-        rt.sync()
 
     def barrier():
         if dist:
             dist.barrier()
         torch.cuda.synchronize()
 
-    kern_ms = []
-    barrier()
-    with Clocks(local) as clk:
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(args.steps):
-            rt.enqueue(bd, out)
-            rt.sync()
-            kern_ms.append(rt.stats()["gpu_ms"])
-        e1.record(stream)
-        barrier()
-    ms = e0.elapsed_time(e1) / args.steps
-    st = rt.stats()
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = ncol * world / (ms / 1e3)
+    def max_over_ranks(x):
+        if dist:
+            t = torch.tensor([x], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            return float(t.item())
+        return x
+
+    bd = {k: (torch.from_numpy(np.ascontiguousarray(v)).to(dev) if isinstance(v, np.ndarray) else v)
+          for k, v in b.items()}
+    precs = ["fp64", "mixed"] if args.precision == "both" else [args.precision]
+    res, outs, handles = {}, {}, {}
+    clk_summary = None
+    for pname in precs:
+        prec = abi.MIXED if pname == "mixed" else abi.FP64
+        rt = abi.Radiation(d, max_layers=48, precision=prec, device=local, validate=False)
+        handles[pname] = rt
+        outs[pname] = abi.alloc_outputs(ncol, L, device=dev)
+        head = pname == precs[-1]   # the headline arm samples clocks
+        with Clocks(local) as clk:
+            ms, kern_ms, st = time_device(rt, bd, outs[pname], args.steps, args.warmup, stream, barrier)
+        if head:
+            clk_summary = clk.summary()
+        ms = max_over_ranks(ms)
+        res[pname] = {"value": ncol * world / (ms / 1e3), "ms_per_step": ms,
+                      "kernel_ms": statistics.mean(kern_ms), "stats": st}
+    hp = precs[-1]
+    rt = handles[hp]
 
     # ---- end to end through the C ABI with pinned host buffers (e2e)
     e2e = None
     if not args.no_e2e:
-        hb = {}
-        keep = []
+        hb, keep = {}, []
         for k, v in b.items():
             if isinstance(v, np.ndarray):
                 tpin = torch.empty(v.shape, dtype=torch.float64, pin_memory=True)
@@ -260,55 +390,74 @@ def main():
             else:
                 hb[k] = v
         ho = {k: torch.empty(tuple(v.shape), dtype=torch.float64, pin_memory=True).numpy()
-              for k, v in out.items()}
+              for k, v in outs[hp].items()}
         h2d = sum(v.nbytes for k, v in hb.items() if isinstance(v, np.ndarray))
         d2h = sum(v.nbytes for v in ho.values()) + hb["detau"].nbytes + hb["cumtauv"].nbytes
+        rt.set_stream(stream)
         for _ in range(args.warmup):
             rt.run(hb, ho, inplace=True)
         barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for _ in range(args.steps):
             rt.run(hb, ho, inplace=True)
         e1.record(stream)
         barrier()
-        ems = e0.elapsed_time(e1) / args.steps
-        if dist:
-            t = torch.tensor([ems], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ems = float(t.item())
+        ems = max_over_ranks(e0.elapsed_time(e1) / args.steps)
         e2e = {"value": ncol * world / (ems / 1e3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
-               "d2h_bytes_per_step": int(d2h), "ms_per_step": ems}
+               "d2h_bytes_per_step": int(d2h), "ms_per_step": ems,
+               "path": f"mgcm_rt_run ({hp}), pinned host buffers"}
+
+    acc = None
+    if "fp64" in outs and "mixed" in outs:
+        acc = accuracy(bd, outs["mixed"], outs["fp64"], L)
+
+    srv = None
+    if not args.no_serving and world == 1 and rank == 0:
+        rt.set_stream(None)
+        srv = serving(rt, dev, seed=77)
 
     if rank == 0:
-        bpc = algorithmic_bytes_per_column(wl["L"], wl["cloud"])
-        kms = statistics.mean(kern_ms)
+        bpc = algorithmic_bytes_per_column(L, wl["cloud"])
+        kms = res[hp]["kernel_ms"]
         ach = bpc * ncol / (kms / 1e3) / 1e9
         pk, pk_kind = peaks()
+        st = res[hp]["stats"]
         line = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64" if prec == abi.FP64 else "f32+f64",
+            "metric": METRIC, "value": res[hp]["value"], "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": res[hp]["ms_per_step"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if hp == "fp64" else "f32+f64",
             "data": "synthetic (seeded, reference input recipe; real k tables)" if kind == "real"
                     else "synthetic (seeded; synthetic k tables)",
-            "config": {"workload": wl["name"], "columns_per_gpu": ncol, "layers": wl["L"],
-                       "precision": args.precision, "k_tables": kind,
+            "config": {"workload": wl["name"], "columns_per_gpu": ncol, "layers": L,
+                       "precision": hp, "k_tables": kind,
                        "l2": "inputs 2.5 GB per step > 126 MB L2 (no flush needed)",
                        "parallelism": f"column shards x{world}, no collective"},
             "gpu_launches": args.steps * int(st["kernels"]),
             "roofline": {"bound": "hbm", "achieved": ach, "peak": pk, "unit": "GB/s",
-                         "frac": ach / pk, "traffic": None,
-                         "kernel": "rt_fp64_kernel" if prec == abi.FP64 else "rt_mixed_kernel",
+                         "frac": ach / pk, "traffic": traffic_per_step(hp, ncol),
+                         "kernel": "radiation pipeline (stage, screen, 2 solves, reduce) per call",
                          "bytes_per_column": bpc, "kernel_ms": kms, "peak_kind": pk_kind},
             "systems_per_step": st["systems"],
-            "clocks": clk.summary(),
+            "clocks": clk_summary,
         }
+        if "fp64" in res and hp != "fp64":
+            line["fp64"] = {"value": res["fp64"]["value"], "ms_per_step": res["fp64"]["ms_per_step"]}
+            line["mixed_vs_fp64"] = res[hp]["value"] / res["fp64"]["value"]
+        if acc:
+            line["accuracy"] = acc
+        if srv:
+            line["serving"] = srv
         if e2e:
             line["e2e"] = e2e
         if not args.no_cpu_baseline and world == 1:
             line["cpu_baseline"] = cpu_baseline(b, d)
         print(json.dumps(line), flush=True)
-    rt.set_stream(None)
-    rt.close()
+    for h in handles.values():
+        h.set_stream(None)
+        h.close()
     if dist:
         dist.destroy_process_group()
 

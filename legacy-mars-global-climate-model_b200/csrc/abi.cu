@@ -385,6 +385,29 @@ void slot_free(mgcm_rt_handle *h, Slot &s) {
     if (s.stream) cudaStreamDestroy(s.stream);
 }
 
+// Function attributes are process-wide per device, so they are set once, to
+// the largest value any layer count or handle needs, never per launch: a
+// per-launch value set by one slot or handle would undercut another's launch.
+int configure_kernels(int device) {
+    static std::mutex mu;
+    static bool done[256] = {};
+    std::lock_guard<std::mutex> lk(mu);
+    if (device < 0 || device >= 256) return MGCM_RT_EINVAL;
+    if (done[device]) return MGCM_RT_OK;
+    size_t rmax = 0;
+    for (int nl = 1; nl <= D_MAXNL; ++nl)
+        rmax = std::max(rmax, reduce_smem_bytes(nl, reduce_rows_per_chunk(nl)));
+    CK(cudaFuncSetAttribute(rt_fp64_reduce, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rmax));
+    CK(cudaFuncSetAttribute(rt_fp64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_CAP));
+    // the solvers use no shared memory: the whole unified L1 goes to the
+    // per-system arrays
+    for (const void *f : {(const void *)rt_fp64_solve<true>, (const void *)rt_fp64_solve<false>,
+                          (const void *)rt_mixed_solve<true>, (const void *)rt_mixed_solve<false>})
+        CK(cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, 0));
+    done[device] = true;
+    return MGCM_RT_OK;
+}
+
 size_t pipe_bytes_per_col(int max_nl, size_t *stride_out = nullptr) {
     const size_t stride = (col_smem_bytes(max_nl, false) + 255) / 256 * 256;
     if (stride_out) *stride_out = stride;
@@ -429,7 +452,6 @@ int launch_pipeline(mgcm_rt_handle *h, Slot &sl, cudaStream_t st, int total, int
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&e, rt_stage, STAGE_THREADS, 0);
         sl.occ_stage = std::max(e, 1);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, rt_fp64_solve<false>, 128, 0);
-        cudaFuncSetAttribute(rt_fp64_reduce, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rsm);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, rt_fp64_reduce, REDUCE_THREADS, rsm);
         sl.occ_screen = std::max(a, 1);
         sl.occ_solve = std::max(b, 1);
@@ -827,6 +849,7 @@ mgcm_rt_handle *mgcm_rt_create(const mgcm_rt_config *cfg, const char *data_dir, 
     if (cudaSetDevice(h->device) != cudaSuccess) { *status = MGCM_RT_ECUDA; return nullptr; }
     cudaDeviceProp prop;
     if (cudaGetDeviceProperties(&prop, h->device) != cudaSuccess) { *status = MGCM_RT_ECUDA; return nullptr; }
+    if (const int rc = configure_kernels(h->device)) { *status = rc; return nullptr; }
     h->num_sms = prop.multiProcessorCount;
     auto fail = [&](int code) { mgcm_rt_destroy(h.release()); *status = code; return nullptr; };
     for (int i = 0; i < 2; ++i) {
@@ -1090,9 +1113,6 @@ extern "C" int mgcm_rt_run_noalloc(mgcm_rt_handle *h, const mgcm_rt_batch_in *in
     const size_t nslab = (MGCM_RT_NOALLOC_SCRATCH_BYTES - NOALLOC_HDR) / slab;
     if (nslab < 1) return MGCM_RT_ENOMEM;
     const size_t smem = col_smem_bytes(max_nl, false);
-    if (cudaFuncSetAttribute(rt_fp64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem) != cudaSuccess)
-        return MGCM_RT_ECUDA;
     int nb = 1;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, rt_fp64_kernel, BLOCK, smem) != cudaSuccess)
         nb = 1;

@@ -17,9 +17,12 @@ struct Lay {   // per-layer two-stream coefficients
     double gama, e1, e2, e3, e4, cp, cm, cpm1, cmm1;
 };
 
+// Per-system arrays (1-based layer index).  Pass A fills a0..a4; pass C
+// writes the layer's two-stream coefficients over the pass-A slots it has
+// consumed (plus c5), and the DSOLVER rows' AS/DS for the back-substitution.
 struct SysLocal {
     double a0[D_MAXNL + 1], a1[D_MAXNL + 1], a2[D_MAXNL + 1], a3[D_MAXNL + 2], a4[D_MAXNL + 1];
-    double c0[D_MAXNL + 1], c1[D_MAXNL + 1], c2[D_MAXNL + 1], c3[D_MAXNL + 1];
+    double c5[D_MAXNL + 1];
     double as[2 * D_MAXNL + 1], ds[2 * D_MAXNL + 1];
 };
 
@@ -31,15 +34,19 @@ __device__ __forceinline__ void elim(double af, double bf, double cf, double df,
     ds = (df - cf * ds1) * x;
 }
 
-// Rows 2n+1 (odd) and 2n (even) of DSOLVER for layers lo = n, hi = n+1.
-__device__ __forceinline__ void elim_pair(const Lay &lo, const Lay &hi, int n, SysLocal &w) {
+// Rows 2n+1 (odd) and 2n (even) of DSOLVER for layers lo = n, hi = n+1; as/ds
+// carry row 2n+2 in and row 2n out, every row is stored for the back-substitution.
+__device__ __forceinline__ void elim_pair(const Lay &lo, const Lay &hi, int n, SysLocal &w,
+                                          double &as, double &ds) {
     {
         const int i = 2 * n + 1;
         const double af = 2.0 * (1.0 - lo.gama * lo.gama);
         const double bf = (lo.e1 - lo.e3) * (1.0 + hi.gama);
         const double cf = (lo.e1 + lo.e3) * (hi.gama - 1.0);
         const double df = lo.e3 * (hi.cpm1 - lo.cp) + lo.e1 * (lo.cm - hi.cmm1);
-        elim(af, bf, cf, df, w.as[i + 1], w.ds[i + 1], w.as[i], w.ds[i]);
+        elim(af, bf, cf, df, as, ds, as, ds);
+        w.as[i] = as;
+        w.ds[i] = ds;
     }
     {
         const int i = 2 * n;
@@ -47,23 +54,28 @@ __device__ __forceinline__ void elim_pair(const Lay &lo, const Lay &hi, int n, S
         const double bf = (lo.e2 + lo.e4) * (hi.gama - 1.0);
         const double cf = 2.0 * (1.0 - hi.gama * hi.gama);
         const double df = (hi.gama - 1.0) * (hi.cpm1 - lo.cp) + (1.0 - hi.gama) * (lo.cm - hi.cmm1);
-        elim(af, bf, cf, df, w.as[i + 1], w.ds[i + 1], w.as[i], w.ds[i]);
+        elim(af, bf, cf, df, as, ds, as, ds);
+        w.as[i] = as;
+        w.ds[i] = ds;
     }
 }
 
 __device__ __forceinline__ void bottom_row(const Lay &b, int nl, double bsurf, double rsf,
-                                           SysLocal &w) {
+                                           SysLocal &w, double &as, double &ds) {
     const int i = 2 * nl;
     const double af = b.e1 - rsf * b.e3;
     const double bf = b.e2 - rsf * b.e4;
     const double df = bsurf - b.cp + rsf * b.cm;
-    w.as[i] = af / bf;
-    w.ds[i] = df / bf;
+    as = af / bf;
+    ds = df / bf;
+    w.as[i] = as;
+    w.ds[i] = ds;
 }
 
-__device__ __forceinline__ void top_row(const Lay &t, double btop, SysLocal &w) {
+__device__ __forceinline__ void top_row(const Lay &t, double btop, SysLocal &w, double as2,
+                                        double ds2) {
     const double af = 0.0, bf = t.gama + 1.0, cf = t.gama - 1.0, df = btop - t.cmm1;
-    elim(af, bf, cf, df, w.as[2], w.ds[2], w.as[1], w.ds[1]);
+    elim(af, bf, cf, df, as2, ds2, w.as[1], w.ds[1]);
 }
 
 // XK(2n-1), XK(2n) -> XK1, XK2 with the underflow test of dsolver.f90:91-101.
@@ -197,10 +209,10 @@ __device__ void solve_vis(const SegDev &sg, int c, int nw, int ng, int sidx, Col
     const double s3 = (double)sqrtf(3.0f), s3h = (double)(sqrtf(3.0f) * 0.5f);
     const double bsurf = rsf * u0 * sg.sol[nw - 1] * mgcm_rt_exp(-dmin(detau / u0, MAXEXP));
     const double btop = 0.0;
-    // c0 = LAMDA, c1 = GAMA, c2 = AM, c3 = AP
-    auto coef = [&](int l, double et_top, double et_bot) {
+    // LAMDA, GAMA, AM overwrite W0, COSBAR, DTAU of the same layer; AP -> c5
+    double *LAM = w.a0, *GAM = w.a1, *AM = w.a2, *AP = w.c5;
+    auto coef = [&](int l, double w0, double cb, double dtl, double et_top, double et_bot) {
         Lay y;
-        const double w0 = w.a0[l], cb = w.a1[l];
         const double g1 = s3h * (2.0 - w0 * (1.0 + cb));
         const double g2 = (s3 * w0 * 0.5) * (1.0 - cb);
         const double g3 = 0.5 * (1.0 - s3 * cb * u0);
@@ -211,15 +223,15 @@ __device__ void solve_vis(const SegDev &sg, int c, int nw, int ng, int sidx, Col
         if (denom == 0.0) denom = R4(1.E-10);
         const double am = f0pi * w0 * (g4 * (g1 + rcp_u0) + g2 * g3) / denom;
         const double ap = f0pi * w0 * (g3 * (g1 - rcp_u0) + g2 * g4) / denom;
-        w.c0[l] = lam;
-        w.c1[l] = y.gama;
-        w.c2[l] = am;
-        w.c3[l] = ap;
+        LAM[l] = lam;
+        GAM[l] = y.gama;
+        AM[l] = am;
+        AP[l] = ap;
         y.cpm1 = ap * et_top;
         y.cmm1 = am * et_top;
         y.cp = ap * et_bot;
         y.cm = am * et_bot;
-        const double ep = mgcm_rt_exp(dmin(TAUMAX, lam * w.a2[l]));
+        const double ep = mgcm_rt_exp(dmin(TAUMAX, lam * dtl));
         const double em = 1.0 / ep;
         y.e1 = ep + y.gama * em;
         y.e2 = ep - y.gama * em;
@@ -229,26 +241,52 @@ __device__ void solve_vis(const SegDev &sg, int c, int nw, int ng, int sidx, Col
     };
     double et_bot = mgcm_rt_exp(-dmin(w.a3[NL + 1] / u0, MAXEXP));
     double et_top = mgcm_rt_exp(-dmin(w.a3[NL] / u0, MAXEXP));
-    Lay hi = coef(NL, et_top, et_bot);
-    bottom_row(hi, NL, bsurf, rsf, w);
+    // layer NL-1's inputs are fetched one step ahead
+    double pw0 = w.a0[NL - 1], pcb = w.a1[NL - 1], pdt = w.a2[NL - 1], pa3 = w.a3[NL - 1];
+    Lay hi = coef(NL, w.a0[NL], w.a1[NL], w.a2[NL], et_top, et_bot);
+    double as, ds;
+    bottom_row(hi, NL, bsurf, rsf, w, as, ds);
     for (int n = NL - 1; n >= 1; --n) {
+        const double w0 = pw0, cb = pcb, dtl = pdt, a3n = pa3;
+        if (n > 1) {
+            pw0 = w.a0[n - 1];
+            pcb = w.a1[n - 1];
+            pdt = w.a2[n - 1];
+            pa3 = w.a3[n - 1];
+        }
         et_bot = et_top;
-        et_top = mgcm_rt_exp(-dmin(w.a3[n] / u0, MAXEXP));
-        const Lay lo = coef(n, et_top, et_bot);
-        elim_pair(lo, hi, n, w);
+        et_top = mgcm_rt_exp(-dmin(a3n / u0, MAXEXP));
+        const Lay lo = coef(n, w0, cb, dtl, et_top, et_bot);
+        elim_pair(lo, hi, n, w, as, ds);
         hi = lo;
     }
-    top_row(hi, btop, w);
+    top_row(hi, btop, w, as, ds);
 
-    // pass D: back-substitution, unmixing, midpoint fluxes.
+    // pass D: back-substitution, unmixing, midpoint fluxes (layer n+1's
+    // values fetched one step ahead).
     double xprev = 0.0;
+    double nas1 = w.as[1], nds1 = w.ds[1], nas2 = w.as[2], nds2 = w.ds[2];
+    double nlam = LAM[1], ngam = GAM[1], nam = AM[1], nap = AP[1], na3 = w.a3[1], na4 = w.a4[1];
     for (int n = 1; n <= NL; ++n) {
-        const double xa = n == 1 ? w.ds[1] : w.ds[2 * n - 1] - w.as[2 * n - 1] * xprev;
-        const double xb = w.ds[2 * n] - w.as[2 * n] * xa;
+        const double as1 = nas1, ds1 = nds1, as2 = nas2, ds2 = nds2;
+        const double lam = nlam, gama = ngam, am = nam, ap = nap, a3n = na3, a4n = na4;
+        if (n < NL) {
+            nas1 = w.as[2 * n + 1];
+            nds1 = w.ds[2 * n + 1];
+            nas2 = w.as[2 * n + 2];
+            nds2 = w.ds[2 * n + 2];
+            nlam = LAM[n + 1];
+            ngam = GAM[n + 1];
+            nam = AM[n + 1];
+            nap = AP[n + 1];
+            na3 = w.a3[n + 1];
+            na4 = w.a4[n + 1];
+        }
+        const double xa = n == 1 ? ds1 : ds1 - as1 * xprev;
+        const double xb = ds2 - as2 * xa;
         xprev = xb;
         double xk1, xk2;
         unmix(xa, xb, xk1, xk2);
-        const double lam = w.c0[n], gama = w.c1[n], am = w.c2[n], ap = w.c3[n];
         if (n == 1) {
             const double ep = 1.0, em = 1.0;
             const double fup = xk1 * ep + gama * xk2 * em + ap;
@@ -258,18 +296,19 @@ __device__ void solve_vis(const SegDev &sg, int c, int nw, int ng, int sidx, Col
             *sc1 = fdn;
         }
         if (n < NL) {
-            const double tcE = n == 1 ? tcE1 : w.a3[n];
-            const double ep = mgcm_rt_exp(dmin(TAUMAX, lam * (w.a4[n] - tcE)));
+            const double tcE = n == 1 ? tcE1 : a3n;
+            const double ep = mgcm_rt_exp(dmin(TAUMAX, lam * (a4n - tcE)));
             const double em = 1.0 / ep;
-            const double et = mgcm_rt_exp(-dmin(w.a4[n] / u0, MAXEXP));
+            const double et = mgcm_rt_exp(-dmin(a4n / u0, MAXEXP));
             const double cpmid = ap * et, cmmid = am * et;
             fmp[n - 1] = xk1 * ep + gama * xk2 * em + cpmid;
             double m = xk1 * ep * gama + xk2 * em + cmmid;
             fmm[n - 1] = m + u0 * f0pi * et;
         } else {
-            const double ep = mgcm_rt_exp(dmin(TAUMAX, lam * (w.a3[NL + 1] - w.a3[NL])));
+            const double tb = w.a3[NL + 1];
+            const double ep = mgcm_rt_exp(dmin(TAUMAX, lam * (tb - a3n)));
             const double em = 1.0 / ep;
-            const double taumid = dmin(w.a3[NL + 1], TAUMAX);
+            const double taumid = dmin(tb, TAUMAX);
             const double et = mgcm_rt_exp(-dmin(taumid / u0, MAXEXP));
             const double cpmid = ap * et, cmmid = am * et;
             fmp[n - 1] = xk1 * ep + gama * xk2 * em + cpmid;
@@ -348,10 +387,11 @@ __device__ void solve_ir(const SegDev &sg, int c, int nw, int ng, int sidx, ColS
     const double tautop = w.a2[1] * plev[2 - 1] / (plev[4 - 1] - plev[2 - 1]);
     const double btop = (1.0 - mgcm_rt_exp(-tautop / UBARI)) * s.pltop_i[nw - 1];
     const double bsurf = s.bsurf_i[nw - 1];
-    // c0 = LAMDA, c1 = GAMA, c2 = B1, c3 = TERM
-    auto coef = [&](int l) {
+    // LAMDA -> a0 (over WBARI), GAMA -> a1, B1 -> c5, TERM -> a3 (a1, a3 unused by pass A)
+    double *LAM = w.a0, *GAM = w.a1, *B1 = w.c5, *TERM = w.a3;
+    auto coef = [&](int l, double w0, double dt) {
         Lay y;
-        const double w0 = w.a0[l], cb = s.cosb_i[l * D_NI + nw - 1], dt = w.a2[l];
+        const double cb = s.cosb_i[l * D_NI + nw - 1];
         const double alpha = sqrt((1.0 - w0) / (1.0 - w0 * cb));
         const double lam = alpha * (1.0 - w0 * cb) / UBARI;
         const double b0 = s.b0_i[l * D_NI + nw - 1];
@@ -368,31 +408,52 @@ __device__ void solve_ir(const SegDev &sg, int c, int nw, int ng, int sidx, ColS
         y.e2 = ep - y.gama * em;
         y.e3 = y.gama * ep + em;
         y.e4 = y.gama * ep - em;
-        w.c0[l] = lam;
-        w.c1[l] = y.gama;
-        w.c2[l] = b1;
-        w.c3[l] = term;
+        LAM[l] = lam;
+        GAM[l] = y.gama;
+        B1[l] = b1;
+        TERM[l] = term;
         return y;
     };
-    Lay hi = coef(NL);
-    bottom_row(hi, NL, bsurf, rsf, w);
+    double pw0 = w.a0[NL - 1], pdt = w.a2[NL - 1];
+    Lay hi = coef(NL, w.a0[NL], w.a2[NL]);
+    double as, ds;
+    bottom_row(hi, NL, bsurf, rsf, w, as, ds);
     for (int n = NL - 1; n >= 1; --n) {
-        const Lay lo = coef(n);
-        elim_pair(lo, hi, n, w);
+        const double w0 = pw0, dt = pdt;
+        if (n > 1) {
+            pw0 = w.a0[n - 1];
+            pdt = w.a2[n - 1];
+        }
+        const Lay lo = coef(n, w0, dt);
+        elim_pair(lo, hi, n, w, as, ds);
         hi = lo;
     }
-    top_row(hi, btop, w);
+    top_row(hi, btop, w, as, ds);
 
     double xprev = 0.0;
+    double nas1 = w.as[1], nds1 = w.ds[1], nas2 = w.as[2], nds2 = w.ds[2];
+    double nlam = LAM[1], ngam = GAM[1], nb1 = B1[1], nterm = TERM[1];
+    double ndtk = 1 < NL ? w.a4[1] : w.a2[1];
     for (int n = 1; n <= NL; ++n) {
-        const double xa = n == 1 ? w.ds[1] : w.ds[2 * n - 1] - w.as[2 * n - 1] * xprev;
-        const double xb = w.ds[2 * n] - w.as[2 * n] * xa;
+        const double as1 = nas1, ds1 = nds1, as2 = nas2, ds2 = nds2;
+        const double lam = nlam, gama = ngam, b1 = nb1, term = nterm, dtk = ndtk;
+        if (n < NL) {
+            nas1 = w.as[2 * n + 1];
+            nds1 = w.ds[2 * n + 1];
+            nas2 = w.as[2 * n + 2];
+            nds2 = w.ds[2 * n + 2];
+            nlam = LAM[n + 1];
+            ngam = GAM[n + 1];
+            nb1 = B1[n + 1];
+            nterm = TERM[n + 1];
+            ndtk = n + 1 < NL ? w.a4[n + 1] : w.a2[n + 1];
+        }
+        const double xa = n == 1 ? ds1 : ds1 - as1 * xprev;
+        const double xb = ds2 - as2 * xa;
         xprev = xb;
         double xk1, xk2;
         unmix(xa, xb, xk1, xk2);
-        const double lam = w.c0[n], gama = w.c1[n], b1 = w.c2[n], term = w.c3[n];
         const double b0 = s.b0_i[n * D_NI + nw - 1];
-        const double dtk = n < NL ? w.a4[n] : w.a2[n];
         const double ep = mgcm_rt_exp(dmin(lam * dtk, TAUMAX));
         const double em = 1.0 / ep;
         const double cpmid = b0 + b1 * dtk + b1 * term;

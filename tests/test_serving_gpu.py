@@ -53,3 +53,24 @@ def test_wait_timeout_and_unknown_ticket(data_dir):
         assert e.value.code == -10
     finally:
         rt.close()
+
+
+def test_layer_counts_alternating_across_slots(data_dir):
+    """Slots that ran different layer counts before must launch any other
+    count: kernel attributes are per function, not per slot."""
+    rt = abi.Radiation(data_dir, max_layers=48, precision=abi.MIXED, validate=False)
+    try:
+        seq = [(20000, 36), (20000, 24), (8000, 36), (20000, 48), (8000, 36), (3000, 24)]
+        batches = [synth.make_batch(n, L=L, seed=60 + i, cloud=True) for i, (n, L) in enumerate(seq)]
+        first = [to_numpy(rt.run(b)) for b in batches]
+        tickets = [rt.submit(_device(b)) for b in batches[::-1]]
+        for (t, out), b, ref in zip(tickets, batches[::-1], first[::-1]):
+            rt.wait(t, 60.0)
+            err = compare(b, to_numpy(out), ref, 1e-12)
+            assert max(err.values()) <= 1e-12, err
+        again = [to_numpy(rt.run(b)) for b in batches]
+        for b, x, y in zip(batches, first, again):
+            err = compare(b, x, y, 1e-12)
+            assert max(err.values()) <= 1e-12, err
+    finally:
+        rt.close()
