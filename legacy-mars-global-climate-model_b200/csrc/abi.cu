@@ -43,20 +43,19 @@ __global__ void rt_fp64_screen(const SegTable *__restrict__ st, int col_begin, i
                                const double *__restrict__ kv, const double *__restrict__ ki,
                                const RtConst K, int *__restrict__ list_v, int *__restrict__ list_i,
                                unsigned int *counts, unsigned long long *nsys,
-                               const float *__restrict__ kvf, const float *__restrict__ kif);
+                               const float *__restrict__ kvf);
 template <bool VIS>
 __global__ void rt_fp64_solve(const SegTable *__restrict__ st, int col_begin, int max_nl,
                               unsigned char *__restrict__ blocks, size_t stride,
                               const double *__restrict__ ktab, const RtConst K,
                               const int *__restrict__ list, const unsigned int *count,
                               double *__restrict__ fl, double *__restrict__ sc);
-template <bool VIS>
-__global__ void rt_mixed_solve(const SegTable *__restrict__ st, int col_begin, int max_nl,
-                               unsigned char *__restrict__ blocks, size_t stride,
-                               const float *__restrict__ ktabf, const double *__restrict__ ktab,
-                               const RtConst K, const int *__restrict__ list,
-                               const unsigned int *count, double *__restrict__ fl,
-                               double *__restrict__ sc);
+__global__ void rt_mixed_solve_vis(const SegTable *__restrict__ st, int col_begin, int max_nl,
+                                   unsigned char *__restrict__ blocks, size_t stride,
+                                   const float *__restrict__ ktabf, const double *__restrict__ ktab,
+                                   const RtConst K, const int *__restrict__ list,
+                                   const unsigned int *count, double *__restrict__ fl,
+                                   double *__restrict__ sc);
 __global__ void rt_fp64_reduce(const SegTable *__restrict__ st, int col_begin, int col_end,
                                int max_nl, unsigned char *__restrict__ blocks, size_t stride,
                                const RtConst K, const double *__restrict__ fl_v,
@@ -176,7 +175,7 @@ struct mgcm_rt_handle {
     HostTables host;
     RtConst K{};
     double *d_kv = nullptr, *d_ki = nullptr, *d_planck = nullptr;
-    float *d_kvf = nullptr, *d_kif = nullptr;
+    float *d_kvf = nullptr;   // FP32 visible table (Cmk*k) of the MIXED path
     std::mutex mu;                                  // serialises the synchronous API
     std::vector<std::unique_ptr<Slot>> slots;       // [0], [1]: synchronous calls
     cudaStream_t user_stream = nullptr;             // mgcm_rt_set_stream
@@ -402,7 +401,7 @@ int configure_kernels(int device) {
     // the solvers use no shared memory: the whole unified L1 goes to the
     // per-system arrays
     for (const void *f : {(const void *)rt_fp64_solve<true>, (const void *)rt_fp64_solve<false>,
-                          (const void *)rt_mixed_solve<true>, (const void *)rt_mixed_solve<false>})
+                          (const void *)rt_mixed_solve_vis})
         CK(cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, 0));
     done[device] = true;
     return MGCM_RT_OK;
@@ -470,23 +469,21 @@ int launch_pipeline(mgcm_rt_handle *h, Slot &sl, cudaStream_t st, int total, int
         if (mixed)
             rt_fp64_screen<true><<<g1, SCREEN_THREADS, 0, st>>>(sl.d_segs, c0, c1, max_nl, blocks, stride,
                                                                 h->d_kv, h->d_ki, h->K, list_v, list_i,
-                                                                counts, sl.d_nsys, h->d_kvf, h->d_kif);
+                                                                counts, sl.d_nsys, h->d_kvf);
         else
             rt_fp64_screen<false><<<g1, SCREEN_THREADS, 0, st>>>(sl.d_segs, c0, c1, max_nl, blocks, stride,
                                                                  h->d_kv, h->d_ki, h->K, list_v, list_i,
-                                                                 counts, sl.d_nsys, nullptr, nullptr);
+                                                                 counts, sl.d_nsys, nullptr);
         const int g2 = h->num_sms * sl.occ_solve;
-        if (mixed) {
-            rt_mixed_solve<true><<<g2, 128, 0, st>>>(sl.d_segs, c0, max_nl, blocks, stride, h->d_kvf,
-                                                     h->d_kv, h->K, list_v, counts, fl_v, sc_v);
-            rt_mixed_solve<false><<<g2, 128, 0, st>>>(sl.d_segs, c0, max_nl, blocks, stride, h->d_kif,
-                                                      h->d_ki, h->K, list_i, counts, fl_i, sc_i);
-        } else {
-            rt_fp64_solve<true><<<g2, 128, 0, st>>>(sl.d_segs, c0, max_nl, blocks, stride, h->d_kv,
-                                                    h->K, list_v, counts, fl_v, sc_v);
-            rt_fp64_solve<false><<<g2, 128, 0, st>>>(sl.d_segs, c0, max_nl, blocks, stride, h->d_ki,
-                                                     h->K, list_i, counts, fl_i, sc_i);
-        }
+        // MIXED: FP32 visible opacities; the IR family is FP64 in both modes
+        if (mixed)
+            rt_mixed_solve_vis<<<g2, 128, 0, st>>>(sl.d_segs, c0, max_nl, blocks, stride, h->d_kvf, h->d_kv,
+                                                   h->K, list_v, counts, fl_v, sc_v);
+        else
+            rt_fp64_solve<true><<<g2, 128, 0, st>>>(sl.d_segs, c0, max_nl, blocks, stride, h->d_kv, h->K,
+                                                    list_v, counts, fl_v, sc_v);
+        rt_fp64_solve<false><<<g2, 128, 0, st>>>(sl.d_segs, c0, max_nl, blocks, stride, h->d_ki, h->K,
+                                                 list_i, counts, fl_i, sc_i);
         const int g3 = std::min((c1 - c0 + REDUCE_WARPS - 1) / REDUCE_WARPS, h->num_sms * sl.occ_reduce);
         rt_fp64_reduce<<<g3, REDUCE_THREADS, rsm, st>>>(sl.d_segs, c0, c1, max_nl, blocks, stride, h->K,
                                                         fl_v, sc_v, fl_i, sc_i, sl.d_status, rb);
@@ -873,17 +870,15 @@ mgcm_rt_handle *mgcm_rt_create(const mgcm_rt_config *cfg, const char *data_dir, 
     gauss_fastest(h->host, kv, ki);
     // FP32 tables hold Cmk*k (optical depth per mbar): k itself reaches 1e-49,
     // below the FP32 range (code/optcv.f90:241-242, U = Cmk*DPR)
-    std::vector<float> kvf(kv.size()), kif(ki.size());
+    std::vector<float> kvf(kv.size());
     for (size_t q = 0; q < kv.size(); ++q) kvf[q] = (float)(3.51e22 * kv[q]);
-    for (size_t q = 0; q < ki.size(); ++q) kif[q] = (float)(3.51e22 * ki[q]);
     if (cudaMalloc(&h->d_kv, kv.size() * 8) || cudaMalloc(&h->d_ki, ki.size() * 8) ||
-        cudaMalloc(&h->d_kvf, kvf.size() * 4) || cudaMalloc(&h->d_kif, kif.size() * 4) ||
+        cudaMalloc(&h->d_kvf, kvf.size() * 4) ||
         cudaMalloc(&h->d_planck, h->host.planckir.size() * 8))
         return fail(MGCM_RT_ENOMEM);
     if (cudaMemcpy(h->d_kv, kv.data(), kv.size() * 8, cudaMemcpyHostToDevice) ||
         cudaMemcpy(h->d_ki, ki.data(), ki.size() * 8, cudaMemcpyHostToDevice) ||
         cudaMemcpy(h->d_kvf, kvf.data(), kvf.size() * 4, cudaMemcpyHostToDevice) ||
-        cudaMemcpy(h->d_kif, kif.data(), kif.size() * 4, cudaMemcpyHostToDevice) ||
         cudaMemcpy(h->d_planck, h->host.planckir.data(), h->host.planckir.size() * 8, cudaMemcpyHostToDevice))
         return fail(MGCM_RT_ECUDA);
     size_t freeb = 0, totb = 0;
@@ -909,7 +904,6 @@ void mgcm_rt_destroy(mgcm_rt_handle *h) {
     cudaFree(h->d_kv);
     cudaFree(h->d_ki);
     cudaFree(h->d_kvf);
-    cudaFree(h->d_kif);
     cudaFree(h->d_planck);
     if (h->fork) cudaEventDestroy(h->fork);
     if (h->join0) cudaEventDestroy(h->join0);

@@ -100,7 +100,8 @@ rt_stage(const SegTable *__restrict__ st, int col_begin, int col_end, int max_nl
 }
 
 // K1: screen every system (optics sums, TLIMIT test, DETAU, CUMTAUV) and
-// append the kept ones to the family lists.  One warp per (column, group);
+// append the kept ones to the family lists.  F32 (mixed precision): visible
+// gas opacities from the FP32 table; the IR family always screens in FP64.  One warp per (column, group);
 // warps never wait on one another.  A group's kept systems take one
 // contiguous run of list positions in ascending order; its base and count go
 // to the column's meta words.
@@ -110,7 +111,7 @@ rt_fp64_screen(const SegTable *__restrict__ st, int col_begin, int col_end, int 
                unsigned char *__restrict__ blocks, size_t stride, const double *__restrict__ kv,
                const double *__restrict__ ki, const RtConst K, int *__restrict__ list_v,
                int *__restrict__ list_i, unsigned int *counts, unsigned long long *nsys,
-               const float *__restrict__ kvf, const float *__restrict__ kif) {
+               const float *__restrict__ kvf) {
     SysLocal w;
     unsigned int nsolved = 0;
     const int lane = threadIdx.x & 31;
@@ -132,8 +133,8 @@ rt_fp64_screen(const SegTable *__restrict__ st, int col_begin, int col_end, int 
             }
         } else if (t < group_end(grp)) {
             const int j = t - NSYS_V;
-            solve_ir<1, F32>(sg, c, j / D_NG + 1, j % D_NG + 1, t, s, K, ki, w, nsolved, nullptr, nullptr,
-                             nullptr, kif);
+            solve_ir<1>(sg, c, j / D_NG + 1, j % D_NG + 1, t, s, K, ki, w, nsolved, nullptr, nullptr,
+                        nullptr);
             act = s.skip[t] == 0;
         }
         const unsigned m = __ballot_sync(0xffffffffu, act);
@@ -157,8 +158,7 @@ rt_fp64_screen(const SegTable *__restrict__ st, int col_begin, int col_end, int 
 #define SCREEN_ARGS                                                                                    \
     const SegTable *__restrict__, int, int, int, unsigned char *__restrict__, size_t,                \
         const double *__restrict__, const double *__restrict__, const RtConst, int *__restrict__,    \
-        int *__restrict__, unsigned int *, unsigned long long *, const float *__restrict__,          \
-        const float *__restrict__
+        int *__restrict__, unsigned int *, unsigned long long *, const float *__restrict__
 template __global__ void rt_fp64_screen<false>(SCREEN_ARGS);
 template __global__ void rt_fp64_screen<true>(SCREEN_ARGS);
 #undef SCREEN_ARGS

@@ -320,11 +320,10 @@ __device__ void solve_vis(const SegDev &sg, int c, int nw, int ng, int sidx, Col
 }
 
 // ---------------------------------------------------------------- infrared
-template <int MODE, bool F32 = false>
+template <int MODE>
 __device__ void solve_ir(const SegDev &sg, int c, int nw, int ng, int sidx, ColSmem &s,
                          const RtConst &K, const double *__restrict__ ki, SysLocal &w,
-                         unsigned int &nsolved, double *fmp, double *fmm, double *sc0,
-                         const float *__restrict__ kif = nullptr) {
+                         unsigned int &nsolved, double *fmp, double *fmm, double *sc0) {
     const int L = sg.L, NL = L + 1, LEV = 2 * L + 3;
     const double fz0 = K.fzeroi[nw - 1];
     if (ng < D_NG && fz0 >= R4(0.99)) {
@@ -332,12 +331,11 @@ __device__ void solve_ir(const SegDev &sg, int c, int nw, int ng, int sidx, ColS
         return;
     }
     const double *tb = ki + (size_t)(nw - 1) * D_NT * D_NP * D_NH * D_NGK + (ng - 1);
-    const float *tbf = F32 ? kif + (size_t)(nw - 1) * D_NT * D_NP * D_NH * D_NGK + (ng - 1) : nullptr;
     double taugsurf = 0.0;
     auto dtauk = [&](int k) -> double {
         const double ta = s.taer_i[k * D_NI + nw - 1], tcl = s.tcld_i[k * D_NI + nw - 1];
         if (ng < D_NG) {
-            const double tg = F32 ? (double)taugas_f(s, k, tbf) : taugas_at(s, k, tb);
+            const double tg = taugas_at(s, k, tb);
             taugsurf += tg;
             return tg + ta + tcl;
         }
