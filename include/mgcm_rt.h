@@ -157,6 +157,36 @@ int mgcm_rt_poll(mgcm_rt_handle *h, long long ticket);
  * returns the request's status and releases the ticket. */
 int mgcm_rt_wait(mgcm_rt_handle *h, long long ticket, double timeout_s);
 
+/* ---- captured uneven batches ------------------------------------------
+ * A fixed set of device-resident batches (e.g. the members of an ensemble,
+ * grids of different layer counts) captured once as a CUDA graph and
+ * replayed every radiation step.  No reference counterpart: the reference
+ * runs one grid per process.  Creation (optionally) autotunes the launch
+ * shape on a sample of the columns, sizes the scratch, then captures;
+ * launches of one graph must be ordered on one stream, and the batch
+ * arrays it was created with must stay allocated. */
+typedef struct mgcm_rt_graph mgcm_rt_graph;
+typedef struct mgcm_rt_tune {
+    int chunk_cols;        /* columns per pipeline pass */
+    int solve_ctas_per_sm; /* solver CTAs per SM (0 = as many as fit) */
+    int reduce_rows;       /* kept-system rows per TMA chunk of the reduce */
+    int candidates;        /* launch shapes timed by the autotuner */
+    int tuning_cols;       /* columns of the tuning sample */
+    double default_ms;     /* built-in shape on the sample */
+    double best_ms;        /* chosen shape on the sample */
+    int kernels;           /* kernel launches in the captured graph */
+    int columns;           /* columns of all batches */
+} mgcm_rt_tune;
+int mgcm_rt_graph_create(mgcm_rt_handle *h, int nbatch, const mgcm_rt_batch_in *in,
+                         mgcm_rt_batch_out *out, int autotune, mgcm_rt_graph **graph);
+/* Enqueues one replay on `stream` (a cudaStream_t; NULL: the graph's own). */
+int mgcm_rt_graph_launch(mgcm_rt_graph *g, void *stream);
+/* Status of the last replay; call after the replay's stream has completed. */
+int mgcm_rt_graph_status(mgcm_rt_graph *g);
+int mgcm_rt_graph_info(const mgcm_rt_graph *g, mgcm_rt_tune *info);
+/* Destroy every graph before its handle. */
+void mgcm_rt_graph_destroy(mgcm_rt_graph *g);
+
 /* Partial radiation between full calls: DNVFLUX = DNDIFFV + direct beam from
  * DETAU (code/dsolflux.f:28-45, code/comp3.f:320-351). */
 int mgcm_rt_dsolflux(mgcm_rt_handle *h, int ncol, int device_ptrs, const double *sol,

@@ -153,6 +153,14 @@ struct Job {
     int seg = 0, c0 = 0, c1 = 0;   // columns [c0, c1) of batch `seg`
 };
 
+// Launch shape of the pipeline; 0 = the built-in choice.  Picked per graph by
+// the autotuner (mgcm_rt_graph_create).
+struct Tune {
+    int chunk = 0;        // columns per pipeline pass
+    int solve_ctas = 0;   // solver CTAs per SM
+    int rb = 0;           // reduce: kept-system rows per TMA chunk
+};
+
 struct Slot {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, done = nullptr;
@@ -160,10 +168,11 @@ struct Slot {
     uint32_t *d_status = nullptr, *h_status = nullptr;
     unsigned long long *d_nsys = nullptr, *h_nsys = nullptr;
     Arena stage, pipe, red;
-    int occ_nl = 0, occ_stage = 1, occ_screen = 1, occ_solve = 1, occ_reduce = 1;
+    int occ_nl = 0, occ_rb = 0, occ_stage = 1, occ_screen = 1, occ_solve = 1, occ_reduce = 1;
     bool busy = false;
     Job job;
     int kernels = 0;
+    Tune tune;
 };
 
 }  // namespace
@@ -393,10 +402,7 @@ int configure_kernels(int device) {
     std::lock_guard<std::mutex> lk(mu);
     if (device < 0 || device >= 256) return MGCM_RT_EINVAL;
     if (done[device]) return MGCM_RT_OK;
-    size_t rmax = 0;
-    for (int nl = 1; nl <= D_MAXNL; ++nl)
-        rmax = std::max(rmax, reduce_smem_bytes(nl, reduce_rows_per_chunk(nl)));
-    CK(cudaFuncSetAttribute(rt_fp64_reduce, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rmax));
+    CK(cudaFuncSetAttribute(rt_fp64_reduce, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_CAP));
     CK(cudaFuncSetAttribute(rt_fp64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_CAP));
     // the solvers use no shared memory: the whole unified L1 goes to the
     // per-system arrays
@@ -423,6 +429,7 @@ int launch_pipeline(mgcm_rt_handle *h, Slot &sl, cudaStream_t st, int total, int
     const size_t per_col = pipe_bytes_per_col(max_nl, &stride);
     const size_t row = (size_t)2 * max_nl * sizeof(double);
     int chunk = std::min(total, max_chunk);
+    if (sl.tune.chunk > 0) chunk = std::min(chunk, sl.tune.chunk);
     const size_t n_v = (size_t)chunk * NSYS_V, n_i = (size_t)chunk * NSYS_I;
     const size_t need = al((size_t)chunk * stride) + al(n_v * 4) + al(n_i * 4) + al(n_v * row) +
                         al(n_i * row) + al(n_v * 32) + al(n_i * 32) + 256;
@@ -439,11 +446,12 @@ int launch_pipeline(mgcm_rt_handle *h, Slot &sl, cudaStream_t st, int total, int
     double *sc_v = reinterpret_cast<double *>(take(n_v * 32));
     double *sc_i = reinterpret_cast<double *>(take(n_i * 32));
     unsigned int *counts = reinterpret_cast<unsigned int *>(take(256));
-    const int rb = reduce_rows_per_chunk(max_nl);
+    const int rb = sl.tune.rb > 0 ? sl.tune.rb : reduce_rows_per_chunk(max_nl);
     const size_t rsm = reduce_smem_bytes(max_nl, rb);
     const bool mixed = h->cfg.precision == MGCM_RT_MIXED;
-    if (sl.occ_nl != max_nl) {
+    if (sl.occ_nl != max_nl || sl.occ_rb != rb) {
         sl.occ_nl = max_nl;
+        sl.occ_rb = rb;
         int a = 1, b = 1, c = 1;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, mixed ? rt_fp64_screen<true> : rt_fp64_screen<false>,
                                                       SCREEN_THREADS, 0);
@@ -454,7 +462,6 @@ int launch_pipeline(mgcm_rt_handle *h, Slot &sl, cudaStream_t st, int total, int
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, rt_fp64_reduce, REDUCE_THREADS, rsm);
         sl.occ_screen = std::max(a, 1);
         sl.occ_solve = std::max(b, 1);
-        if (const char *e = std::getenv("MGCM_RT_SOLVE_CTAS_PER_SM")) sl.occ_solve = std::max(1, std::atoi(e));
         sl.occ_reduce = std::max(c, 1);
     }
     for (int c0 = 0; c0 < total; c0 += chunk) {
@@ -474,7 +481,7 @@ int launch_pipeline(mgcm_rt_handle *h, Slot &sl, cudaStream_t st, int total, int
             rt_fp64_screen<false><<<g1, SCREEN_THREADS, 0, st>>>(sl.d_segs, c0, c1, max_nl, blocks, stride,
                                                                  h->d_kv, h->d_ki, h->K, list_v, list_i,
                                                                  counts, sl.d_nsys, nullptr);
-        const int g2 = h->num_sms * sl.occ_solve;
+        const int g2 = h->num_sms * (sl.tune.solve_ctas > 0 ? sl.tune.solve_ctas : sl.occ_solve);
         // MIXED: FP32 visible opacities; the IR family is FP64 in both modes
         if (mixed)
             rt_mixed_solve_vis<<<g2, 128, 0, st>>>(sl.d_segs, c0, max_nl, blocks, stride, h->d_kvf, h->d_kv,
@@ -1052,6 +1059,203 @@ int mgcm_rt_wait(mgcm_rt_handle *h, long long ticket, double timeout_s) {
     }
     h->reqs.erase(ticket);
     return r->status;
+}
+}
+
+// ---------------------------------------------------------------------------
+// Captured uneven batches: segment table built once, launch shape autotuned,
+// the pipeline captured into a CUDA graph on the graph's own slot.
+struct mgcm_rt_graph {
+    mgcm_rt_handle *h = nullptr;
+    Slot slot;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int total = 0, max_nl = 1, max_chunk = 1;
+    mgcm_rt_tune info{};
+};
+
+namespace {
+
+// One eager pass over the first `cols` columns with shape t; returns ms.
+int time_shape(mgcm_rt_graph *g, const Tune &t, int cols, float &ms) {
+    mgcm_rt_handle *h = g->h;
+    Slot &sl = g->slot;
+    cudaStream_t st = sl.stream;
+    sl.tune = t;
+    int nk = 0;
+    float best = 1e30f;
+    for (int rep = 0; rep < 2; ++rep) {
+        CK(cudaMemsetAsync(sl.d_status, 0, 256, st));
+        CK(cudaEventRecord(sl.ev0, st));
+        int rc = launch_pipeline(h, sl, st, cols, g->max_nl, nk, g->max_chunk);
+        if (rc) return rc;
+        CK(cudaEventRecord(sl.ev1, st));
+        CK(cudaStreamSynchronize(st));
+        float x = 0.f;
+        cudaEventElapsedTime(&x, sl.ev0, sl.ev1);
+        best = std::min(best, x);
+    }
+    ms = best;
+    return MGCM_RT_OK;
+}
+
+void graph_free(mgcm_rt_graph *g) {
+    if (!g) return;
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    if (g->graph) cudaGraphDestroy(g->graph);
+    if (g->h) slot_free(g->h, g->slot);
+    delete g;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mgcm_rt_graph_create(mgcm_rt_handle *h, int nbatch, const mgcm_rt_batch_in *in,
+                         mgcm_rt_batch_out *out, int autotune, mgcm_rt_graph **graph) {
+    if (!h || !in || !out || !graph || nbatch < 1 || nbatch > MAX_SEGS) return MGCM_RT_EINVAL;
+    *graph = nullptr;
+    std::lock_guard<std::mutex> lk(h->mu);
+    if (cudaSetDevice(h->device) != cudaSuccess) return MGCM_RT_ECUDA;
+    for (int b = 0; b < nbatch; ++b) {
+        const int rc = check_args(h, &in[b], &out[b]);
+        if (rc) return rc;
+        if (!in[b].device_ptrs) return MGCM_RT_EINVAL;
+    }
+    mgcm_rt_graph *g = new mgcm_rt_graph;
+    g->h = h;
+    auto fail = [&](int code) { graph_free(g); return code; };
+    if (slot_init(g->slot)) return fail(MGCM_RT_ECUDA);
+    Slot &sl = g->slot;
+    SegTable &tab = *sl.h_segs;
+    tab.nseg = 0;
+    int total = 0, max_nl = 1;
+    for (int b = 0; b < nbatch; ++b) {
+        const Sizes z = sizes_of(in[b]);
+        if (z.ncol == 0) continue;
+        if ((long long)total + (long long)z.ncol > 0x7fffff) return fail(MGCM_RT_EINVAL);
+        SegDev sd{};
+        sd.ncol = (int)z.ncol;
+        sd.L = z.L;
+        sd.col0 = total;
+        sd.ptrop = in[b].ptrop;
+        fill_direct(sd, in[b], out[b]);
+        sd.sigma = in[b].sigma;
+        sd.sol = in[b].sol;
+        tab.seg[tab.nseg++] = sd;
+        max_nl = std::max(max_nl, z.nl);
+        total += (int)z.ncol;
+    }
+    if (total == 0) return fail(MGCM_RT_EINVAL);
+    tab.total_cols = total;
+    if (cudaMemcpyAsync(sl.d_segs, sl.h_segs, sizeof(SegTable), cudaMemcpyHostToDevice, sl.stream) ||
+        cudaStreamSynchronize(sl.stream))
+        return fail(MGCM_RT_ECUDA);
+    g->total = total;
+    g->max_nl = max_nl;
+    const size_t per_col = pipe_bytes_per_col(max_nl);
+    g->max_chunk = (int)std::max<size_t>(1, std::min<size_t>(total, (h->budget / 4) / per_col));
+
+    // autotune: coordinate descent over chunk, solver CTAs per SM and reduce
+    // rows per chunk, each shape timed (best of two) on the first columns
+    Tune best{};
+    const int sample = std::min(total, 131072);
+    float t_def = 0.f;
+    int rc = time_shape(g, best, sample, t_def);
+    if (rc) return fail(rc);
+    rc = time_shape(g, best, sample, t_def);   // the first pass also sized the scratch
+    if (rc) return fail(rc);
+    float t_best = t_def;
+    int ncand = 1;
+    if (autotune) {
+        auto consider = [&](Tune t) -> int {
+            float ms = 0.f;
+            const int r = time_shape(g, t, sample, ms);
+            if (r) return r;
+            ++ncand;
+            if (ms < t_best) {
+                t_best = ms;
+                best = t;
+            }
+            return MGCM_RT_OK;
+        };
+        for (int c : {16384, 32768, 65536}) {
+            if (c >= sample || c > g->max_chunk) continue;
+            Tune t = best;
+            t.chunk = c;
+            if ((rc = consider(t))) return fail(rc);
+        }
+        for (int k : {2, 3, 4, 5, 6}) {
+            Tune t = best;
+            t.solve_ctas = k;
+            if ((rc = consider(t))) return fail(rc);
+        }
+        for (int r : {1, 2, 4, 8}) {
+            if (reduce_smem_bytes(max_nl, r) > SMEM_CAP) continue;
+            if (r == reduce_rows_per_chunk(max_nl)) continue;
+            Tune t = best;
+            t.rb = r;
+            if ((rc = consider(t))) return fail(rc);
+        }
+    }
+    sl.tune = best;
+    // one eager pass over every column with the chosen shape sizes the
+    // scratch for the capture (nothing may allocate while capturing)
+    float t_full = 0.f;
+    if ((rc = time_shape(g, best, total, t_full))) return fail(rc);
+
+    int nk = 0;
+    cudaStream_t st = sl.stream;
+    if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return fail(MGCM_RT_ECUDA);
+    int crc = MGCM_RT_OK;
+    if (cudaMemsetAsync(sl.d_status, 0, 256, st) != cudaSuccess) crc = MGCM_RT_ECUDA;
+    if (!crc) crc = launch_pipeline(h, sl, st, total, max_nl, nk, g->max_chunk);
+    if (!crc) crc = post_status(sl, st);
+    cudaGraph_t gr = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(st, &gr);
+    if (crc || ce != cudaSuccess || !gr) {
+        if (gr) cudaGraphDestroy(gr);
+        return fail(crc ? crc : MGCM_RT_ECUDA);
+    }
+    g->graph = gr;
+    if (cudaGraphInstantiate(&g->exec, gr, 0) != cudaSuccess) return fail(MGCM_RT_ECUDA);
+    mgcm_rt_tune &inf = g->info;
+    inf.chunk_cols = best.chunk > 0 ? std::min(best.chunk, g->max_chunk) : std::min(total, g->max_chunk);
+    inf.solve_ctas_per_sm = best.solve_ctas;
+    inf.reduce_rows = best.rb > 0 ? best.rb : reduce_rows_per_chunk(max_nl);
+    inf.candidates = ncand;
+    inf.tuning_cols = sample;
+    inf.default_ms = t_def;
+    inf.best_ms = t_best;
+    inf.kernels = nk;
+    inf.columns = total;
+    *graph = g;
+    return MGCM_RT_OK;
+}
+
+int mgcm_rt_graph_launch(mgcm_rt_graph *g, void *stream) {
+    if (!g || !g->exec) return MGCM_RT_EINVAL;
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : g->slot.stream;
+    CK(cudaGraphLaunch(g->exec, st));
+    return MGCM_RT_OK;
+}
+
+int mgcm_rt_graph_status(mgcm_rt_graph *g) {
+    if (!g) return MGCM_RT_EINVAL;
+    return status_to_code(*g->slot.h_status);
+}
+
+int mgcm_rt_graph_info(const mgcm_rt_graph *g, mgcm_rt_tune *info) {
+    if (!g || !info) return MGCM_RT_EINVAL;
+    *info = g->info;
+    return MGCM_RT_OK;
+}
+
+void mgcm_rt_graph_destroy(mgcm_rt_graph *g) {
+    if (!g) return;
+    std::lock_guard<std::mutex> lk(g->h->mu);
+    cudaSetDevice(g->h->device);
+    graph_free(g);
 }
 }
 

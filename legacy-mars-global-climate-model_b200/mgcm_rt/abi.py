@@ -59,6 +59,12 @@ class RTError(RuntimeError):
         super().__init__(f"{where}: {STATUS.get(code, code)} ({lib().mgcm_rt_strerror(code).decode()})")
 
 
+class Tune(C.Structure):
+    _fields_ = [("chunk_cols", C.c_int), ("solve_ctas_per_sm", C.c_int), ("reduce_rows", C.c_int),
+                ("candidates", C.c_int), ("tuning_cols", C.c_int), ("default_ms", C.c_double),
+                ("best_ms", C.c_double), ("kernels", C.c_int), ("columns", C.c_int)]
+
+
 _lib = None
 
 
@@ -87,6 +93,12 @@ def lib():
         L.mgcm_rt_strerror.restype = C.c_char_p
         L.mgcm_rt_strerror.argtypes = [C.c_int]
         L.mgcm_rt_version.restype = C.c_char_p
+        L.mgcm_rt_graph_create.argtypes = [C.c_void_p, C.c_int, C.POINTER(BatchIn), C.POINTER(BatchOut),
+                                           C.c_int, C.POINTER(C.c_void_p)]
+        L.mgcm_rt_graph_launch.argtypes = [C.c_void_p, C.c_void_p]
+        L.mgcm_rt_graph_status.argtypes = [C.c_void_p]
+        L.mgcm_rt_graph_info.argtypes = [C.c_void_p, C.POINTER(Tune)]
+        L.mgcm_rt_graph_destroy.argtypes = [C.c_void_p]
         _lib = L
     return _lib
 
@@ -244,6 +256,29 @@ class Radiation:
             o["cumtauv"] = b["cumtauv"]
         return outs
 
+    # ---- captured uneven batches --------------------------------------
+    def graph(self, batches: list, outs: list | None = None, autotune: bool = True) -> "Graph":
+        """Capture device-resident batches (one per grid or ensemble member, up
+        to 64) as one CUDA graph; see Graph."""
+        for b in batches:
+            if not (_is_torch(b["plev"]) and b["plev"].is_cuda):
+                raise ValueError("graph batches must be CUDA tensors")
+        keep: list = []
+        ins = (BatchIn * len(batches))()
+        if outs is None:
+            outs = [alloc_outputs(int(b["ncol"]), int(b["L"]), device=b["plev"].device) for b in batches]
+        outs_c = (BatchOut * len(batches))()
+        for i, b in enumerate(batches):
+            ins[i] = make_in(b, True, keep)
+            outs_c[i] = make_out(outs[i])
+        g = C.c_void_p()
+        rc = lib().mgcm_rt_graph_create(self._h, len(batches), ins, outs_c, 1 if autotune else 0, C.byref(g))
+        if rc != 0:
+            raise RTError(rc, "mgcm_rt_graph_create")
+        for b, o in zip(batches, outs):
+            o["detau"], o["cumtauv"] = b["detau"], b["cumtauv"]
+        return Graph(self, g, outs, (keep, ins, outs_c, batches))
+
     # ---- serving -------------------------------------------------------
     def submit(self, b: dict, out: dict | None = None) -> tuple[int, dict]:
         """Queue batch ``b``; returns (ticket, out).  Arrays must stay alive and
@@ -312,6 +347,35 @@ def tables_host(data_dir) -> dict:
     if rc != 0:
         raise RTError(rc, "mgcm_rt_tables_host")
     return {"co2v": co2v, "co2i": co2i, "planckir": pl, "pfgasref": pf}
+
+
+class Graph:
+    """A captured set of batches: launch(stream) replays the whole radiation
+    call of every batch; results land in .outs (DETAU/CUMTAUV in the batches)."""
+
+    def __init__(self, rt: Radiation, g, outs, keep):
+        self._rt, self._g, self.outs, self._keep = rt, g, outs, keep
+
+    def launch(self, stream=None) -> None:
+        ptr = None if stream is None else int(getattr(stream, "cuda_stream", stream))
+        rc = lib().mgcm_rt_graph_launch(self._g, ptr)
+        if rc != 0:
+            raise RTError(rc, "mgcm_rt_graph_launch")
+
+    def status(self) -> int:
+        return lib().mgcm_rt_graph_status(self._g)
+
+    def info(self) -> dict:
+        t = Tune()
+        rc = lib().mgcm_rt_graph_info(self._g, C.byref(t))
+        if rc != 0:
+            raise RTError(rc, "mgcm_rt_graph_info")
+        return {k: getattr(t, k) for k, _ in Tune._fields_}
+
+    def close(self) -> None:
+        if self._g:
+            lib().mgcm_rt_graph_destroy(self._g)
+            self._g = None
 
 
 def exported_symbols() -> list[str]:
