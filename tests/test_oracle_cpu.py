@@ -205,3 +205,21 @@ def test_shared_exp_accuracy():
         same += a == b
     assert same / len(xs) > 0.99
     assert L.orc_exp(0.0) == 1.0
+
+
+@pytest.mark.parametrize("name", ["c1_l24_cloud", "c0_l36_dust"])
+def test_oracle_reproduces_golden_vectors(otables, name):
+    """The oracle and the input recipe reproduce the committed fixtures
+    (tests/golden/make_golden.py)."""
+    import importlib.util
+    import pathlib
+    gdir = pathlib.Path(__file__).parent / "golden"
+    spec = importlib.util.spec_from_file_location("make_golden", gdir / "make_golden.py")
+    mg = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mg)
+    g = np.load(gdir / f"{name}.npz")
+    b = mg.case(name)
+    assert mg.inputs_digest(b) == str(g["digest"]), "input recipe changed"
+    out = oracle.run_batch(otables, b)
+    for k, v in out.items():
+        np.testing.assert_allclose(np.asarray(v), g[k], rtol=1e-13, atol=1e-300, err_msg=k)
