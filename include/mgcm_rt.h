@@ -72,7 +72,14 @@ typedef struct {
     int device;           /* CUDA device ordinal */
     int validate;         /* nonzero: check inputs (finite, T range) before each launch */
     size_t hbm_budget;    /* device bytes for batch staging; 0 = 3/4 of free memory */
+    int solver;           /* MGCM_RT_SOLVER_AUTO / _THREAD: one thread per (band, Gauss)
+                             system; MGCM_RT_SOLVER_QUAD: four lanes per system with the
+                             per-layer values in registers (L <= 51; same results) */
 } mgcm_rt_config;
+
+#define MGCM_RT_SOLVER_AUTO 0
+#define MGCM_RT_SOLVER_THREAD 1
+#define MGCM_RT_SOLVER_QUAD 2
 
 /* One batch of columns on one vertical grid. */
 typedef struct {
@@ -156,6 +163,29 @@ int mgcm_rt_poll(mgcm_rt_handle *h, long long ticket);
 /* Blocks until the ticket finishes or timeout_s passes (<0: no limit);
  * returns the request's status and releases the ticket. */
 int mgcm_rt_wait(mgcm_rt_handle *h, long long ticket, double timeout_s);
+
+/* ---- tracer inputs: aerosol optics on the device -----------------------
+ * The per-level dust and water-ice optical properties that COMP3 builds on
+ * the host (code/comp3.f:592-630: OPT_DST from the dust tracers, or the
+ * prescribed INI_OPTDST band properties with TAUREF from FILLTAUCUM; OPT_CLD
+ * from the ice tracers) are computed on the device from the tracer mixing
+ * ratios, then the radiation runs as in mgcm_rt_run.  The host passes about
+ * 5 KB per column instead of ~35 KB (L = 24).  No reference counterpart as
+ * one call; the outputs equal mgcm_rt_run on the host-computed arrays. */
+typedef struct {
+    int ncol, nlayers, device_ptrs;
+    int active_dust;     /* 1: OPT_DST from dust_mass, dust_number; 0: prescribed dust, tauref given */
+    int cloudon;         /* 1: OPT_CLD from ice_mass, ice_core_mass, ice_number; 0: no cloud */
+    double ptrop;
+    const double *sigma, *sol;
+    const double *plev, *tlev, *pmid, *tmid, *qh2o;       /* [ncol][2L+3] */
+    const double *tauref;                                 /* [ncol][2L+4] (active_dust = 0) */
+    const double *dust_mass, *dust_number;                /* [ncol][L] QTRACE(J,I,L,iMa_dt/iNb_dt) */
+    const double *ice_mass, *ice_core_mass, *ice_number;  /* [ncol][L] iMa_cld, iMa_cor, iNb_cld */
+    const double *acosz, *als, *albi, *pcol;              /* [ncol] */
+    double *detau, *cumtauv;                              /* [ncol][17][7] in/out */
+} mgcm_rt_batch_tracers;
+int mgcm_rt_run_tracers(mgcm_rt_handle *h, const mgcm_rt_batch_tracers *in, mgcm_rt_batch_out *out);
 
 /* ---- captured uneven batches ------------------------------------------
  * A fixed set of device-resident batches (e.g. the members of an ensemble,

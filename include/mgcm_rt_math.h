@@ -150,4 +150,94 @@ MGCM_RT_HD double mgcm_rt_log10(double x) {
                        MGCM_RT_ADD(MGCM_RT_MUL(ed, L2LO), MGCM_RT_MUL(lnm, LOG10E)));
 }
 
+/* Natural logarithm, the same reduction and series as mgcm_rt_log10:
+ * ln x = e ln2 + 2 atanh(s), ln2 split so that e*hi is exact.  About one ulp;
+ * identical on host and device. */
+MGCM_RT_HD double mgcm_rt_ln(double x) {
+    const double LN2HI = 0x1.62e42fee00000p-1, LN2LO = 0x1.a39ef35793c76p-33;
+    const double SQRT2 = 0x1.6a09e667f3bcdp+0;
+    const double C[11] = {0x1.5555555555555p-2, 0x1.999999999999ap-3, 0x1.2492492492492p-3,
+                          0x1.c71c71c71c71cp-4, 0x1.745d1745d1746p-4, 0x1.3b13b13b13b14p-4,
+                          0x1.1111111111111p-4, 0x1.e1e1e1e1e1e1ep-5, 0x1.af286bca1af28p-5,
+                          0x1.8618618618618p-5, 0x1.642c8590b2164p-5};
+    if (!(x > 0.0)) return x == 0.0 ? -HUGE_VAL : (x - x) / (x - x);
+    if (x == HUGE_VAL) return x;
+    int e = 0;
+    if (x < 0x1.0p-1022) {
+        x = MGCM_RT_MUL(x, 0x1.0p+54);
+        e = -54;
+    }
+    uint64_t bits;
+    memcpy(&bits, &x, sizeof bits);
+    e += (int)((bits >> 52) & 0x7ff) - 1023;
+    bits = (bits & 0x000fffffffffffffull) | 0x3ff0000000000000ull;
+    double m;
+    memcpy(&m, &bits, sizeof m);
+    if (m > SQRT2) {
+        m = MGCM_RT_MUL(m, 0.5);
+        e += 1;
+    }
+    const double f = MGCM_RT_ADD(m, -1.0);
+    const double s = f / MGCM_RT_ADD(2.0, f);
+    const double z = MGCM_RT_MUL(s, s);
+    double r = C[10];
+    for (int k = 9; k >= 0; --k) r = MGCM_RT_ADD(C[k], MGCM_RT_MUL(z, r));
+    r = MGCM_RT_MUL(z, r);
+    const double s2 = MGCM_RT_ADD(s, s);
+    const double lnm = MGCM_RT_ADD(s2, MGCM_RT_MUL(s2, r));
+    const double ed = (double)e;
+    return MGCM_RT_ADD(MGCM_RT_MUL(ed, LN2HI), MGCM_RT_ADD(MGCM_RT_MUL(ed, LN2LO), lnm));
+}
+
+/* x**y for x > 0 as exp(y ln x) (the aerosol optics' real powers,
+ * code/opt_dst.f:110, code/opt_cld.f:129).  Relative error about
+ * (1 + |y ln x|) ulp. */
+MGCM_RT_HD double mgcm_rt_pow(double x, double y) {
+    return mgcm_rt_exp(MGCM_RT_MUL(y, mgcm_rt_ln(x)));
+}
+
+/* Error function (the DERF of the aerosol size-bin weights,
+ * code/opt_dst.f:120-121).  |x| < 1.5: Maclaurin series
+ *   erf x = 2/sqrt(pi) sum_n (-1)^n x^(2n+1) / (n! (2n+1)),
+ * summed until the terms fall below 2^-60 of the sum (at most 60 terms);
+ * 1.5 <= |x| < 6: erf x = 1 - erfc x with the continued fraction
+ *   erfc x = exp(-x^2)/sqrt(pi) / (x + (1/2)/(x + 1/(x + (3/2)/(x + ...)))),
+ * its 100th convergent A/B from the forward three-term recurrences
+ * (A, B stay below 1e100 on this range); |x| >= 6: +-1.
+ * Absolute error below 1e-15; identical on host and device. */
+MGCM_RT_HD double mgcm_rt_erf(double x) {
+    const double TWO_RSQPI = 0x1.20dd750429b6dp+0, RSQPI = 0x1.20dd750429b6dp-1;
+    const double ax = x < 0.0 ? -x : x;
+    double r;
+    if (ax < 1.5) {
+        const double mx2 = -MGCM_RT_MUL(x, x);
+        double t = x, sum = x;
+        for (int n = 1; n <= 60; ++n) {
+            t = MGCM_RT_MUL(t, mx2) / (double)n;
+            const double term = t / (double)(2 * n + 1);
+            sum = MGCM_RT_ADD(sum, term);
+            const double at = term < 0.0 ? -term : term, as = sum < 0.0 ? -sum : sum;
+            if (at < MGCM_RT_MUL(as, 0x1.0p-60)) break;
+        }
+        return MGCM_RT_MUL(TWO_RSQPI, sum);
+    }
+    if (ax >= 6.0) {
+        r = 1.0;
+    } else {
+        double a1 = 1.0, a0 = ax, b1 = 0.0, b0 = 1.0;
+        for (int n = 1; n <= 100; ++n) {
+            const double an = MGCM_RT_MUL(0.5, (double)n);
+            const double a = MGCM_RT_ADD(MGCM_RT_MUL(ax, a0), MGCM_RT_MUL(an, a1));
+            const double b = MGCM_RT_ADD(MGCM_RT_MUL(ax, b0), MGCM_RT_MUL(an, b1));
+            a1 = a0;
+            a0 = a;
+            b1 = b0;
+            b0 = b;
+        }
+        const double erfc = MGCM_RT_MUL(MGCM_RT_MUL(mgcm_rt_exp(-MGCM_RT_MUL(ax, ax)), RSQPI), b0 / a0);
+        r = MGCM_RT_ADD(1.0, -erfc);
+    }
+    return x < 0.0 ? -r : r;
+}
+
 #endif /* MGCM_RT_MATH_H */

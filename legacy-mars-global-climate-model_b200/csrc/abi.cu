@@ -26,6 +26,7 @@
 #include <vector>
 
 #include "../../include/mgcm_rt.h"
+#include "rt_aerosol.cuh"
 #include "rt_column.cuh"
 #include "tables.h"
 
@@ -50,6 +51,17 @@ __global__ void rt_fp64_solve(const SegTable *__restrict__ st, int col_begin, in
                               const double *__restrict__ ktab, const RtConst K,
                               const int *__restrict__ list, const unsigned int *count,
                               double *__restrict__ fl, double *__restrict__ sc);
+template <bool VIS, int R>
+__global__ void rt_quad_solve(const SegTable *__restrict__ st, int col_begin, int max_nl,
+                              unsigned char *__restrict__ blocks, size_t stride,
+                              const double *__restrict__ ktab, const RtConst K, const int *__restrict__ list,
+                              const unsigned int *count, double *__restrict__ fl, double *__restrict__ sc);
+template <int R>
+__global__ void rt_quad_mixed_vis(const SegTable *__restrict__ st, int col_begin, int max_nl,
+                                  unsigned char *__restrict__ blocks, size_t stride,
+                                  const float *__restrict__ ktabf, const double *__restrict__ ktab,
+                                  const RtConst K, const int *__restrict__ list, const unsigned int *count,
+                                  double *__restrict__ fl, double *__restrict__ sc);
 __global__ void rt_mixed_solve_vis(const SegTable *__restrict__ st, int col_begin, int max_nl,
                                    unsigned char *__restrict__ blocks, size_t stride,
                                    const float *__restrict__ ktabf, const double *__restrict__ ktab,
@@ -167,8 +179,8 @@ struct Slot {
     SegTable *h_segs = nullptr, *d_segs = nullptr;
     uint32_t *d_status = nullptr, *h_status = nullptr;
     unsigned long long *d_nsys = nullptr, *h_nsys = nullptr;
-    Arena stage, pipe, red;
-    int occ_nl = 0, occ_rb = 0, occ_stage = 1, occ_screen = 1, occ_solve = 1, occ_reduce = 1;
+    Arena stage, pipe, aero;   // aero: per-level aerosol arrays of tracer jobs
+    int occ_nl = 0, occ_rb = 0, occ_stage = 1, occ_screen = 1, occ_solve = 1, occ_quad = 1, occ_reduce = 1;
     bool busy = false;
     Job job;
     int kernels = 0;
@@ -185,6 +197,9 @@ struct mgcm_rt_handle {
     RtConst K{};
     double *d_kv = nullptr, *d_ki = nullptr, *d_planck = nullptr;
     float *d_kvf = nullptr;   // FP32 visible table (Cmk*k) of the MIXED path
+    bool quad = false;        // four-lane solvers for L <= 51 (mgcm_rt_config.solver)
+    AeroConst aero{};         // aerosol optics constants (mgcm_rt_run_tracers)
+    double *d_mie = nullptr;  // Mie tables on the device; null when the files were absent
     std::mutex mu;                                  // serialises the synchronous API
     std::vector<std::unique_ptr<Slot>> slots;       // [0], [1]: synchronous calls
     cudaStream_t user_stream = nullptr;             // mgcm_rt_set_stream
@@ -334,7 +349,6 @@ void fill_direct(SegDev &sd, const mgcm_rt_batch_in &in, const mgcm_rt_batch_out
     sd.fluxsurf = out.fluxsurf;
 }
 
-bool red_in_smem(int max_nl) { return col_smem_bytes(max_nl, true) <= SMEM_CAP; }
 
 cudaStream_t sync_stream(mgcm_rt_handle *h) {
     return h->user_stream ? h->user_stream : h->slots[0]->stream;
@@ -376,7 +390,7 @@ int slot_init(Slot &s) {
 
 void slot_free(mgcm_rt_handle *h, Slot &s) {
     if (s.stream) cudaStreamSynchronize(s.stream);
-    for (Arena *a : {&s.stage, &s.pipe, &s.red})
+    for (Arena *a : {&s.stage, &s.pipe, &s.aero})
         if (a->ptr) {
             cudaFree(a->ptr);
             h->used -= a->bytes;
@@ -459,6 +473,12 @@ int launch_pipeline(mgcm_rt_handle *h, Slot &sl, cudaStream_t st, int total, int
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&e, rt_stage, STAGE_THREADS, 0);
         sl.occ_stage = std::max(e, 1);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, rt_fp64_solve<false>, 128, 0);
+        int qo = 1;
+        const int qr = quad_r_for(max_nl);
+        if (qr == 7) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&qo, rt_quad_solve<false, 7>, 128, 0);
+        else if (qr == 10) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&qo, rt_quad_solve<false, 10>, 128, 0);
+        else if (qr == 13) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&qo, rt_quad_solve<false, 13>, 128, 0);
+        sl.occ_quad = std::max(qo, 1);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, rt_fp64_reduce, REDUCE_THREADS, rsm);
         sl.occ_screen = std::max(a, 1);
         sl.occ_solve = std::max(b, 1);
@@ -483,14 +503,34 @@ int launch_pipeline(mgcm_rt_handle *h, Slot &sl, cudaStream_t st, int total, int
                                                                  counts, sl.d_nsys, nullptr);
         const int g2 = h->num_sms * (sl.tune.solve_ctas > 0 ? sl.tune.solve_ctas : sl.occ_solve);
         // MIXED: FP32 visible opacities; the IR family is FP64 in both modes
-        if (mixed)
-            rt_mixed_solve_vis<<<g2, 128, 0, st>>>(sl.d_segs, c0, max_nl, blocks, stride, h->d_kvf, h->d_kv,
-                                                   h->K, list_v, counts, fl_v, sc_v);
-        else
-            rt_fp64_solve<true><<<g2, 128, 0, st>>>(sl.d_segs, c0, max_nl, blocks, stride, h->d_kv, h->K,
-                                                    list_v, counts, fl_v, sc_v);
-        rt_fp64_solve<false><<<g2, 128, 0, st>>>(sl.d_segs, c0, max_nl, blocks, stride, h->d_ki, h->K,
-                                                 list_i, counts, fl_i, sc_i);
+        const int qr = h->quad ? quad_r_for(max_nl) : 0;
+        if (qr) {
+            const int gq = h->num_sms * (sl.tune.solve_ctas > 0 ? sl.tune.solve_ctas : sl.occ_quad);
+#define MGCM_QUAD(R)                                                                                        \
+    do {                                                                                                    \
+        if (mixed)                                                                                          \
+            rt_quad_mixed_vis<R><<<gq, 128, 0, st>>>(sl.d_segs, c0, max_nl, blocks, stride, h->d_kvf,        \
+                                                     h->d_kv, h->K, list_v, counts, fl_v, sc_v);             \
+        else                                                                                                \
+            rt_quad_solve<true, R><<<gq, 128, 0, st>>>(sl.d_segs, c0, max_nl, blocks, stride, h->d_kv, h->K, \
+                                                       list_v, counts, fl_v, sc_v);                          \
+        rt_quad_solve<false, R><<<gq, 128, 0, st>>>(sl.d_segs, c0, max_nl, blocks, stride, h->d_ki, h->K,    \
+                                                    list_i, counts, fl_i, sc_i);                             \
+    } while (0)
+            if (qr == 7) MGCM_QUAD(7);
+            else if (qr == 10) MGCM_QUAD(10);
+            else MGCM_QUAD(13);
+#undef MGCM_QUAD
+        } else {
+            if (mixed)
+                rt_mixed_solve_vis<<<g2, 128, 0, st>>>(sl.d_segs, c0, max_nl, blocks, stride, h->d_kvf, h->d_kv,
+                                                       h->K, list_v, counts, fl_v, sc_v);
+            else
+                rt_fp64_solve<true><<<g2, 128, 0, st>>>(sl.d_segs, c0, max_nl, blocks, stride, h->d_kv, h->K,
+                                                        list_v, counts, fl_v, sc_v);
+            rt_fp64_solve<false><<<g2, 128, 0, st>>>(sl.d_segs, c0, max_nl, blocks, stride, h->d_ki, h->K,
+                                                     list_i, counts, fl_i, sc_i);
+        }
         const int g3 = std::min((c1 - c0 + REDUCE_WARPS - 1) / REDUCE_WARPS, h->num_sms * sl.occ_reduce);
         rt_fp64_reduce<<<g3, REDUCE_THREADS, rsm, st>>>(sl.d_segs, c0, c1, max_nl, blocks, stride, h->K,
                                                         fl_v, sc_v, fl_i, sc_i, sl.d_status, rb);
@@ -706,6 +746,224 @@ int run_host(mgcm_rt_handle *h, int nbatch, const mgcm_rt_batch_in *in, mgcm_rt_
     return status_to_code(acc);
 }
 
+// ---------------------------------------------------------------- tracer inputs
+int check_tracers(const mgcm_rt_handle *h, const mgcm_rt_batch_tracers *in, const mgcm_rt_batch_out *out) {
+    if (!h || !in || !out) return MGCM_RT_EINVAL;
+    if (in->ncol < 0) return MGCM_RT_EINVAL;
+    if (in->nlayers < 1 || in->nlayers > MGCM_RT_MAX_LAYERS || in->nlayers > h->cfg.max_layers)
+        return MGCM_RT_ELAYERS;
+    if (in->ncol == 0) return MGCM_RT_OK;
+    const void *req[] = {in->sigma, in->sol, in->plev, in->tlev, in->pmid, in->tmid, in->qh2o,
+                         in->acosz, in->als, in->albi, in->pcol, in->detau, in->cumtauv,
+                         out->fmnetv, out->fluxupv, out->fluxdnv, out->fmneti, out->fluxupi,
+                         out->fluxdni, out->suntot, out->irtotal, out->qrad, out->nfluxtopv,
+                         out->nfluxtopi, out->diffvt, out->dnvflux, out->dndiffv, out->dnirflux,
+                         out->fluxsurf};
+    for (const void *p : req)
+        if (!p) return MGCM_RT_EINVAL;
+    if (in->active_dust ? (!in->dust_mass || !in->dust_number) : !in->tauref) return MGCM_RT_EINVAL;
+    if (in->cloudon && (!in->ice_mass || !in->ice_core_mass || !in->ice_number)) return MGCM_RT_EINVAL;
+    if (!std::isfinite(in->ptrop) || !(in->ptrop > 0.0)) return MGCM_RT_ENONFINITE;
+    if (!h->d_mie) return MGCM_RT_EIO;
+    return MGCM_RT_OK;
+}
+
+// One job of a tracer batch on a slot: compact inputs staged (host) or
+// offset (device), the aerosol arrays filled by rt_aerosol, the pipeline,
+// outputs copied back (host); records sl.done.
+int issue_tracer_job(mgcm_rt_handle *h, Slot &sl, cudaStream_t st, const mgcm_rt_batch_tracers &in,
+                     const mgcm_rt_batch_out &out, int c0, int c1) {
+    const size_t n = (size_t)(c1 - c0);
+    const int L = in.nlayers, lev = 2 * L + 3, lev1 = lev + 1, nl = L + 1;
+    SegDev sd{};
+    sd.ncol = (int)n;
+    sd.L = L;
+    sd.col0 = 0;
+    sd.ptrop = in.ptrop;
+    AeroSeg as{};
+    as.ncol = (int)n;
+    as.L = L;
+    as.active_dust = in.active_dust ? 1 : 0;
+    as.cloudon = in.cloudon ? 1 : 0;
+    std::vector<ArrSpec> arrs;
+    auto add_in = [&](const double *p, size_t per, const double **f) {
+        if (p) arrs.push_back({p, nullptr, per, 0, const_cast<double **>(f)});
+    };
+    auto add_out = [&](double *p, size_t per, double **f) { arrs.push_back({nullptr, p, per, 1, f}); };
+    add_in(in.plev, lev, &sd.plev);
+    add_in(in.tlev, lev, &sd.tlev);
+    add_in(in.pmid, lev, &sd.pmid);
+    add_in(in.tmid, lev, &sd.tmid);
+    add_in(in.qh2o, lev, &sd.qh2o);
+    if (!in.active_dust) add_in(in.tauref, lev1, &as.tauref_in);
+    if (in.active_dust) {
+        add_in(in.dust_mass, L, &as.dust_mass);
+        add_in(in.dust_number, L, &as.dust_number);
+    }
+    if (in.cloudon) {
+        add_in(in.ice_mass, L, &as.ice_mass);
+        add_in(in.ice_core_mass, L, &as.ice_core);
+        add_in(in.ice_number, L, &as.ice_number);
+    }
+    add_in(in.acosz, 1, &sd.acosz);
+    add_in(in.als, 1, &sd.als);
+    add_in(in.albi, 1, &sd.albi);
+    add_in(in.pcol, 1, &sd.pcol);
+    arrs.push_back({in.detau, in.detau, 119, 2, &sd.detau});
+    arrs.push_back({in.cumtauv, in.cumtauv, 119, 2, &sd.cumtauv});
+    add_out(out.fmnetv, nl, &sd.fmnetv);
+    add_out(out.fluxupv, nl, &sd.fluxupv);
+    add_out(out.fluxdnv, nl, &sd.fluxdnv);
+    add_out(out.fmneti, nl, &sd.fmneti);
+    add_out(out.fluxupi, nl, &sd.fluxupi);
+    add_out(out.fluxdni, nl, &sd.fluxdni);
+    add_out(out.suntot, nl, &sd.suntot);
+    add_out(out.irtotal, nl, &sd.irtotal);
+    add_out(out.qrad, nl, &sd.qrad);
+    add_out(out.nfluxtopv, 1, &sd.nfluxtopv);
+    add_out(out.nfluxtopi, 1, &sd.nfluxtopi);
+    add_out(out.diffvt, 1, &sd.diffvt);
+    add_out(out.dnvflux, 1, &sd.dnvflux);
+    add_out(out.dndiffv, 1, &sd.dndiffv);
+    add_out(out.dnirflux, 1, &sd.dnirflux);
+    add_out(out.fluxsurf, 1, &sd.fluxsurf);
+    if (in.device_ptrs) {
+        for (auto &a : arrs) *a.seg_field = const_cast<double *>(a.src ? a.src : a.dst) + (size_t)c0 * a.per_col;
+        sd.sigma = in.sigma;
+        sd.sol = in.sol;
+    } else {
+        size_t bytes = ((lev + 8) * 8 + 255) / 256 * 256;
+        for (const auto &a : arrs) bytes += ((a.per_col * n * 8 + 255) / 256) * 256;
+        const int rc = arena_ensure(h, sl.stage, bytes, st);
+        if (rc) return rc;
+        char *base = static_cast<char *>(sl.stage.ptr);
+        size_t off = 0;
+        for (auto &a : arrs) {
+            double *d = reinterpret_cast<double *>(base + off);
+            off += ((a.per_col * n * 8 + 255) / 256) * 256;
+            *a.seg_field = d;
+            a.dev = d;
+            if (a.dir != 1)
+                CK(cudaMemcpyAsync(d, a.src + (size_t)c0 * a.per_col, a.per_col * n * 8,
+                                   cudaMemcpyHostToDevice, st));
+        }
+        double *ds = reinterpret_cast<double *>(base + off);
+        CK(cudaMemcpyAsync(ds, in.sigma, lev * 8, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(ds + lev, in.sol, 7 * 8, cudaMemcpyHostToDevice, st));
+        sd.sigma = ds;
+        sd.sol = ds + lev;
+    }
+    // the per-level aerosol arrays of the ABI, on the device
+    const size_t per = (size_t)lev1 * (2 + 3 * (AERO_NV + AERO_NI));
+    const size_t abytes = n * per * 8 * (in.cloudon ? 2 : 1);
+    int rc = arena_ensure(h, sl.aero, abytes, st);
+    if (rc) return rc;
+    double *ap = static_cast<double *>(sl.aero.ptr);
+    auto take = [&](size_t per_col) { double *r = ap; ap += per_col * n; return r; };
+    as.tauref = take(lev1);
+    as.qextrefdst = take(lev1);
+    as.qxvdst = take((size_t)AERO_NV * lev1);
+    as.qsvdst = take((size_t)AERO_NV * lev1);
+    as.gvdst = take((size_t)AERO_NV * lev1);
+    as.qxidst = take((size_t)AERO_NI * lev1);
+    as.qsidst = take((size_t)AERO_NI * lev1);
+    as.gidst = take((size_t)AERO_NI * lev1);
+    if (in.cloudon) {
+        as.taurefcld = take(lev1);
+        as.qextrefcld = take(lev1);
+        as.qxvcld = take((size_t)AERO_NV * lev1);
+        as.qsvcld = take((size_t)AERO_NV * lev1);
+        as.gvcld = take((size_t)AERO_NV * lev1);
+        as.qxicld = take((size_t)AERO_NI * lev1);
+        as.qsicld = take((size_t)AERO_NI * lev1);
+        as.gicld = take((size_t)AERO_NI * lev1);
+    }
+    as.plev = sd.plev;
+    sd.tauref = as.tauref;
+    sd.qextrefdst = as.qextrefdst;
+    sd.qxvdst = as.qxvdst;
+    sd.qsvdst = as.qsvdst;
+    sd.gvdst = as.gvdst;
+    sd.qxidst = as.qxidst;
+    sd.qsidst = as.qsidst;
+    sd.gidst = as.gidst;
+    sd.taurefcld = as.taurefcld;
+    sd.qextrefcld = as.qextrefcld;
+    sd.qxvcld = as.qxvcld;
+    sd.qsvcld = as.qsvcld;
+    sd.gvcld = as.gvcld;
+    sd.qxicld = as.qxicld;
+    sd.qsicld = as.qsicld;
+    sd.gicld = as.gicld;
+    SegTable &tab = *sl.h_segs;
+    tab.nseg = 1;
+    tab.total_cols = (int)n;
+    tab.seg[0] = sd;
+    CK(cudaMemcpyAsync(sl.d_segs, sl.h_segs, offsetof(SegTable, seg) + sizeof(SegDev),
+                       cudaMemcpyHostToDevice, st));
+    const long long items = (long long)n * (L + 1);
+    const int ag = (int)std::min<long long>((items + 127) / 128, (long long)h->num_sms * 16);
+    rt_aerosol<<<ag, 128, 0, st>>>(as, h->aero, h->d_mie);
+    CK(cudaGetLastError());
+    rc = launch_all(h, sl, st, (int)n, nl, 1 << 30);
+    if (rc) return rc;
+    ++sl.kernels;
+    if (!in.device_ptrs)
+        for (auto &a : arrs)
+            if (a.dir != 0)
+                CK(cudaMemcpyAsync(a.dst + (size_t)c0 * a.per_col, a.dev, a.per_col * n * 8,
+                                   cudaMemcpyDeviceToHost, st));
+    rc = post_status(sl, st);
+    if (rc) return rc;
+    CK(cudaEventRecord(sl.done, st));
+    return MGCM_RT_OK;
+}
+
+// Synchronous tracer batch: jobs alternate between the two synchronous slots.
+int run_tracers(mgcm_rt_handle *h, const mgcm_rt_batch_tracers &in, mgcm_rt_batch_out &out) {
+    cudaStream_t ust = sync_stream(h);
+    CK(cudaEventRecord(h->fork, ust));
+    for (auto &s : h->slots) CK(cudaStreamWaitEvent(s->stream, h->fork, 0));
+    uint32_t acc = 0;
+    long long systems = 0;
+    int nk = 0, k = 0;
+    bool used[2] = {false, false};
+    const int job = in.device_ptrs ? 4 * SYNC_JOB_COLS : SYNC_JOB_COLS;
+    for (int c0 = 0; c0 < in.ncol; c0 += job, ++k) {
+        const int c1 = std::min(in.ncol, c0 + job);
+        Slot &sl = *h->slots[k & 1];
+        if (used[k & 1]) {
+            CK(cudaEventSynchronize(sl.done));
+            acc |= *sl.h_status;
+            systems += (long long)*sl.h_nsys;
+        }
+        const int rc = issue_tracer_job(h, sl, sl.stream, in, out, c0, c1);
+        if (rc) return rc;
+        used[k & 1] = true;
+        nk += sl.kernels;
+    }
+    for (int i = 0; i < 2; ++i) {
+        Slot &sl = *h->slots[i];
+        if (used[i]) {
+            CK(cudaEventSynchronize(sl.done));
+            acc |= *sl.h_status;
+            systems += (long long)*sl.h_nsys;
+        }
+    }
+    CK(cudaEventRecord(h->join0, h->slots[0]->stream));
+    CK(cudaEventRecord(h->join1, h->slots[1]->stream));
+    CK(cudaStreamWaitEvent(ust, h->join0, 0));
+    CK(cudaStreamWaitEvent(ust, h->join1, 0));
+    float ms = 0.f;
+    if (used[0]) cudaEventElapsedTime(&ms, h->slots[0]->ev0, h->slots[0]->ev1);
+    h->stats.gpu_ms = ms;
+    h->stats.columns = in.ncol;
+    h->stats.systems = systems;
+    h->stats.status = (int)acc;
+    h->stats.kernels = nk;
+    return status_to_code(acc);
+}
+
 int run_batches(mgcm_rt_handle *h, int nbatch, const mgcm_rt_batch_in *in, mgcm_rt_batch_out *out,
                 bool async) {
     if (nbatch < 1 || nbatch > MAX_SEGS) return MGCM_RT_EINVAL;
@@ -854,6 +1112,8 @@ mgcm_rt_handle *mgcm_rt_create(const mgcm_rt_config *cfg, const char *data_dir, 
     cudaDeviceProp prop;
     if (cudaGetDeviceProperties(&prop, h->device) != cudaSuccess) { *status = MGCM_RT_ECUDA; return nullptr; }
     if (const int rc = configure_kernels(h->device)) { *status = rc; return nullptr; }
+    if (cfg->solver < MGCM_RT_SOLVER_AUTO || cfg->solver > MGCM_RT_SOLVER_QUAD) { *status = MGCM_RT_EINVAL; return nullptr; }
+    h->quad = cfg->solver == MGCM_RT_SOLVER_QUAD;
     h->num_sms = prop.multiProcessorCount;
     auto fail = [&](int code) { mgcm_rt_destroy(h.release()); *status = code; return nullptr; };
     for (int i = 0; i < 2; ++i) {
@@ -888,6 +1148,39 @@ mgcm_rt_handle *mgcm_rt_create(const mgcm_rt_config *cfg, const char *data_dir, 
         cudaMemcpy(h->d_kvf, kvf.data(), kvf.size() * 4, cudaMemcpyHostToDevice) ||
         cudaMemcpy(h->d_planck, h->host.planckir.data(), h->host.planckir.size() * 8, cudaMemcpyHostToDevice))
         return fail(MGCM_RT_ECUDA);
+    {   // aerosol optics tables: optional (mgcm_rt_run_tracers returns EIO without them)
+        AerosolTables at;
+        if (load_aerosol_tables(data_dir, at) == 0) {
+            AeroConst &A = h->aero;
+            std::memcpy(A.radb, at.radb, sizeof(A.radb));
+            for (int j = 0; j < AERO_NRATIO; ++j) A.cor_ratio[j] = (float)at.cor_ratio[j];
+            std::memcpy(A.qextv, at.qextv, sizeof(A.qextv));
+            std::memcpy(A.qscatv, at.qscatv, sizeof(A.qscatv));
+            std::memcpy(A.gv, at.gv, sizeof(A.gv));
+            std::memcpy(A.qexti, at.qexti, sizeof(A.qexti));
+            std::memcpy(A.qscati, at.qscati, sizeof(A.qscati));
+            std::memcpy(A.gi, at.gi, sizeof(A.gi));
+            std::vector<double> mie;
+            mie.reserve(AERO_MIE_SIZE);
+            for (int m = 0; m < 3; ++m)
+                for (int i = 0; i < AERO_NBIN; ++i)
+                    for (int l = 0; l < AERO_NV; ++l) mie.push_back(at.dst_v[m][i][l]);
+            for (int m = 0; m < 3; ++m)
+                for (int i = 0; i < AERO_NBIN; ++i)
+                    for (int l = 0; l < AERO_NI; ++l) mie.push_back(at.dst_i[m][i][l]);
+            for (int m = 0; m < 3; ++m)
+                for (int j = 0; j < AERO_NRATIO; ++j)
+                    for (int i = 0; i < AERO_NBIN; ++i)
+                        for (int l = 0; l < AERO_NV; ++l) mie.push_back(at.cld_v[m][j][i][l]);
+            for (int m = 0; m < 3; ++m)
+                for (int j = 0; j < AERO_NRATIO; ++j)
+                    for (int i = 0; i < AERO_NBIN; ++i)
+                        for (int l = 0; l < AERO_NI; ++l) mie.push_back(at.cld_i[m][j][i][l]);
+            if (cudaMalloc(&h->d_mie, mie.size() * 8) ||
+                cudaMemcpy(h->d_mie, mie.data(), mie.size() * 8, cudaMemcpyHostToDevice))
+                return fail(MGCM_RT_ENOMEM);
+        }
+    }
     size_t freeb = 0, totb = 0;
     cudaMemGetInfo(&freeb, &totb);
     h->budget = cfg->hbm_budget ? cfg->hbm_budget : freeb / 4 * 3;
@@ -911,6 +1204,7 @@ void mgcm_rt_destroy(mgcm_rt_handle *h) {
     cudaFree(h->d_kv);
     cudaFree(h->d_ki);
     cudaFree(h->d_kvf);
+    cudaFree(h->d_mie);
     cudaFree(h->d_planck);
     if (h->fork) cudaEventDestroy(h->fork);
     if (h->join0) cudaEventDestroy(h->join0);
@@ -999,6 +1293,16 @@ int mgcm_rt_dsolflux(mgcm_rt_handle *h, int ncol, int device_ptrs, const double 
     if (!device_ptrs) CK(cudaMemcpyAsync(dnvflux, dout, (size_t)ncol * 8, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     return MGCM_RT_OK;
+}
+
+int mgcm_rt_run_tracers(mgcm_rt_handle *h, const mgcm_rt_batch_tracers *in, mgcm_rt_batch_out *out) {
+    const int rc = check_tracers(h, in, out);
+    if (rc || in->ncol == 0) return rc;
+    std::lock_guard<std::mutex> lk(h->mu);
+    if (cudaSetDevice(h->device) != cudaSuccess) return MGCM_RT_ECUDA;
+    const int prc = finish_pending(h);
+    if (prc) return prc;
+    return run_tracers(h, *in, *out);
 }
 
 int mgcm_rt_submit(mgcm_rt_handle *h, const mgcm_rt_batch_in *in, mgcm_rt_batch_out *out,

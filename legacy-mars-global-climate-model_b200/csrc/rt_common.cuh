@@ -27,6 +27,12 @@ __host__ __device__ constexpr int group_end(int w) {
                                       : NSYS);
 }
 
+// Layers per lane of the four-lane solvers for a largest NL (0: NL > 52,
+// the one-thread-per-system solvers run).
+__host__ __device__ constexpr int quad_r_for(int nl) {
+    return nl <= 28 ? 7 : (nl <= 40 ? 10 : (nl <= 52 ? 13 : 0));
+}
+
 // device status bits (OR-ed into the status word)
 constexpr uint32_t ST_PLANCK_RANGE = 1u;   // a Planck index left 1..8501 (clamped)
 constexpr uint32_t ST_NONFINITE = 2u;      // validation: NaN/Inf or p <= 0 in an input

@@ -27,6 +27,7 @@
 // exponential goes through mgcm_rt_exp (include/mgcm_rt_math.h), the routine
 // the CPU oracle uses too, so host and device agree bit-for-bit.
 #include "rt_fp64_sys.cuh"
+#include "rt_quad.cuh"
 #include "rt_tma.cuh"
 #include "../../include/mgcm_rt_math.h"
 
@@ -200,6 +201,51 @@ template __global__ void rt_fp64_solve<false>(const SegTable *__restrict__, int,
                                               size_t, const double *__restrict__, const RtConst,
                                               const int *__restrict__, const unsigned int *,
                                               double *__restrict__, double *__restrict__);
+
+// K2 (four-lane form, L <= 51): a quad of lanes per kept system, 8 systems
+// per warp, per-layer values in registers (rt_quad.cuh).  A quad past the
+// end of the list repeats the last system and stores nothing.
+template <bool VIS, int R>
+__global__ void __launch_bounds__(128)
+rt_quad_solve(const SegTable *__restrict__ st, int col_begin, int max_nl,
+              unsigned char *__restrict__ blocks, size_t stride, const double *__restrict__ ktab,
+              const RtConst K, const int *__restrict__ list, const unsigned int *count,
+              double *__restrict__ fl, double *__restrict__ sc) {
+    const unsigned int n = VIS ? count[0] : count[1];
+    const unsigned int lane = threadIdx.x & 31;
+    const unsigned int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const unsigned int nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (unsigned int base = warp * 8; base < n; base += nwarps * 8) {
+        const unsigned int i = base + (lane >> 2);
+        const bool live = i < n;
+        const unsigned int ii = live ? i : n - 1;
+        const int e = list[ii];
+        const int g = e >> 8, sidx = e & 255;
+        const SegDev &sg = st->seg[find_seg(st, g)];
+        const int c = g - sg.col0;
+        const ColSmem s = carve_smem(blocks + (size_t)(g - col_begin) * stride, max_nl, nullptr, false);
+        double *row = fl + (size_t)ii * 2 * max_nl, *scr = sc + (size_t)ii * 4;
+        if (VIS) {
+            quad_vis<R, false>(sg, c, sidx / D_NG + 1, sidx % D_NG + 1, s, K, ktab, nullptr, live, row,
+                               row + max_nl, scr);
+        } else {
+            const int j = sidx - NSYS_V;
+            quad_ir<R>(sg, c, j / D_NG + 1, j % D_NG + 1, s, K, ktab, live, row, row + max_nl, scr);
+        }
+    }
+}
+
+#define QUAD_ARGS                                                                                      \
+    const SegTable *__restrict__, int, int, unsigned char *__restrict__, size_t, const double *__restrict__, \
+        const RtConst, const int *__restrict__, const unsigned int *, double *__restrict__,             \
+        double *__restrict__
+template __global__ void rt_quad_solve<true, 7>(QUAD_ARGS);
+template __global__ void rt_quad_solve<true, 10>(QUAD_ARGS);
+template __global__ void rt_quad_solve<true, 13>(QUAD_ARGS);
+template __global__ void rt_quad_solve<false, 7>(QUAD_ARGS);
+template __global__ void rt_quad_solve<false, 10>(QUAD_ARGS);
+template __global__ void rt_quad_solve<false, 13>(QUAD_ARGS);
+#undef QUAD_ARGS
 
 // K3: ordered sums and heating, one warp per column.  A column's kept systems
 // sit in contiguous rows of the compact flux buffers (visible, then IR).  Lane

@@ -34,48 +34,67 @@ __device__ __forceinline__ void elim(double af, double bf, double cf, double df,
     ds = (df - cf * ds1) * x;
 }
 
-// Rows 2n+1 (odd) and 2n (even) of DSOLVER for layers lo = n, hi = n+1; as/ds
-// carry row 2n+2 in and row 2n out, every row is stored for the back-substitution.
-__device__ __forceinline__ void elim_pair(const Lay &lo, const Lay &hi, int n, SysLocal &w,
-                                          double &as, double &ds) {
+// Rows 2n+1 (odd) and 2n (even) of DSOLVER for layers lo = n, hi = n+1,
+// eliminated in DTRIDGL's order: as/ds carry row 2n+2 in and row 2n out;
+// row 2n+1 is returned in as_odd/ds_odd.
+__device__ __forceinline__ void rows_of_pair(const Lay &lo, const Lay &hi, double &as, double &ds,
+                                             double &as_odd, double &ds_odd) {
     {
-        const int i = 2 * n + 1;
         const double af = 2.0 * (1.0 - lo.gama * lo.gama);
         const double bf = (lo.e1 - lo.e3) * (1.0 + hi.gama);
         const double cf = (lo.e1 + lo.e3) * (hi.gama - 1.0);
         const double df = lo.e3 * (hi.cpm1 - lo.cp) + lo.e1 * (lo.cm - hi.cmm1);
         elim(af, bf, cf, df, as, ds, as, ds);
-        w.as[i] = as;
-        w.ds[i] = ds;
+        as_odd = as;
+        ds_odd = ds;
     }
     {
-        const int i = 2 * n;
         const double af = (lo.e1 + lo.e3) * (hi.gama - 1.0);
         const double bf = (lo.e2 + lo.e4) * (hi.gama - 1.0);
         const double cf = 2.0 * (1.0 - hi.gama * hi.gama);
         const double df = (hi.gama - 1.0) * (hi.cpm1 - lo.cp) + (1.0 - hi.gama) * (lo.cm - hi.cmm1);
         elim(af, bf, cf, df, as, ds, as, ds);
-        w.as[i] = as;
-        w.ds[i] = ds;
     }
 }
 
-__device__ __forceinline__ void bottom_row(const Lay &b, int nl, double bsurf, double rsf,
-                                           SysLocal &w, double &as, double &ds) {
-    const int i = 2 * nl;
+// The same with every row stored for the back-substitution.
+__device__ __forceinline__ void elim_pair(const Lay &lo, const Lay &hi, int n, SysLocal &w,
+                                          double &as, double &ds) {
+    double ao, dd;
+    rows_of_pair(lo, hi, as, ds, ao, dd);
+    w.as[2 * n + 1] = ao;
+    w.ds[2 * n + 1] = dd;
+    w.as[2 * n] = as;
+    w.ds[2 * n] = ds;
+}
+
+// Row 2NL (surface) of DSOLVER.
+__device__ __forceinline__ void bottom_row_v(const Lay &b, double bsurf, double rsf, double &as,
+                                             double &ds) {
     const double af = b.e1 - rsf * b.e3;
     const double bf = b.e2 - rsf * b.e4;
     const double df = bsurf - b.cp + rsf * b.cm;
     as = af / bf;
     ds = df / bf;
-    w.as[i] = as;
-    w.ds[i] = ds;
+}
+
+// Row 1 (top) of DSOLVER given row 2.
+__device__ __forceinline__ void top_row_v(const Lay &t, double btop, double as2, double ds2, double &as1,
+                                          double &ds1) {
+    const double af = 0.0, bf = t.gama + 1.0, cf = t.gama - 1.0, df = btop - t.cmm1;
+    elim(af, bf, cf, df, as2, ds2, as1, ds1);
+}
+
+__device__ __forceinline__ void bottom_row(const Lay &b, int nl, double bsurf, double rsf,
+                                           SysLocal &w, double &as, double &ds) {
+    bottom_row_v(b, bsurf, rsf, as, ds);
+    w.as[2 * nl] = as;
+    w.ds[2 * nl] = ds;
 }
 
 __device__ __forceinline__ void top_row(const Lay &t, double btop, SysLocal &w, double as2,
                                         double ds2) {
-    const double af = 0.0, bf = t.gama + 1.0, cf = t.gama - 1.0, df = btop - t.cmm1;
-    elim(af, bf, cf, df, as2, ds2, w.as[1], w.ds[1]);
+    top_row_v(t, btop, as2, ds2, w.as[1], w.ds[1]);
 }
 
 // XK(2n-1), XK(2n) -> XK1, XK2 with the underflow test of dsolver.f90:91-101.

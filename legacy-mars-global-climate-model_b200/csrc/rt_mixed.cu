@@ -17,7 +17,7 @@
 // absorption), at or above the 1e-2 K/sol tolerance; the visible family
 // under the same rounding moves heating by 4e-6 K/sol.  FP32 two-stream
 // coefficients put ~0.2 K/sol of rounding noise into the thin top layers.
-#include "rt_fp64_sys.cuh"
+#include "rt_quad.cuh"
 
 namespace mgcm {
 
@@ -40,5 +40,40 @@ rt_mixed_solve_vis(const SegTable *__restrict__ st, int col_begin, int max_nl,
                                  dummy, row, row + max_nl, scr, scr + 1, scr + 2, ktabf);
     }
 }
+
+// Four-lane form (L <= 51), as rt_quad_solve<true, R> with FP32 opacities.
+template <int R>
+__global__ void __launch_bounds__(128)
+rt_quad_mixed_vis(const SegTable *__restrict__ st, int col_begin, int max_nl,
+                  unsigned char *__restrict__ blocks, size_t stride, const float *__restrict__ ktabf,
+                  const double *__restrict__ ktab, const RtConst K, const int *__restrict__ list,
+                  const unsigned int *count, double *__restrict__ fl, double *__restrict__ sc) {
+    const unsigned int n = count[0];
+    const unsigned int lane = threadIdx.x & 31;
+    const unsigned int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const unsigned int nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (unsigned int base = warp * 8; base < n; base += nwarps * 8) {
+        const unsigned int i = base + (lane >> 2);
+        const bool live = i < n;
+        const unsigned int ii = live ? i : n - 1;
+        const int e = list[ii];
+        const int g = e >> 8, sidx = e & 255;
+        const SegDev &sg = st->seg[find_seg(st, g)];
+        const int c = g - sg.col0;
+        const ColSmem s = carve_smem(blocks + (size_t)(g - col_begin) * stride, max_nl, nullptr, false);
+        double *row = fl + (size_t)ii * 2 * max_nl, *scr = sc + (size_t)ii * 4;
+        fp64::quad_vis<R, true>(sg, c, sidx / D_NG + 1, sidx % D_NG + 1, s, K, ktab, ktabf, live, row,
+                                row + max_nl, scr);
+    }
+}
+
+#define QUADM_ARGS                                                                                     \
+    const SegTable *__restrict__, int, int, unsigned char *__restrict__, size_t, const float *__restrict__,  \
+        const double *__restrict__, const RtConst, const int *__restrict__, const unsigned int *,      \
+        double *__restrict__, double *__restrict__
+template __global__ void rt_quad_mixed_vis<7>(QUADM_ARGS);
+template __global__ void rt_quad_mixed_vis<10>(QUADM_ARGS);
+template __global__ void rt_quad_mixed_vis<13>(QUADM_ARGS);
+#undef QUADM_ARGS
 
 }  // namespace mgcm

@@ -10,6 +10,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 
 namespace mgcm {
@@ -188,6 +189,76 @@ int load_tables(const std::string &dir, HostTables &t) {
     const int rc = read_ktables(dir, v8, fv, i8, fi);
     if (rc) return rc;
     build_tables(t, v8, fv, i8, fi);
+    return 0;
+}
+
+// Whitespace-separated REAL*4 values of a formatted Mie table file, as
+// code/initcld.f:161-178 reads them.
+static int read_real4(const std::string &path, std::vector<double> &v, size_t n) {
+    FILE *f = std::fopen(path.c_str(), "r");
+    if (!f) return -1;
+    v.clear();
+    char tok[64];
+    while (v.size() < n && std::fscanf(f, "%63s", tok) == 1) v.push_back((double)std::strtof(tok, nullptr));
+    std::fclose(f);
+    return v.size() == n ? 0 : -2;
+}
+
+int load_aerosol_tables(const std::string &dir, AerosolTables &a) {
+    const auto R4 = [](double x) { return (double)(float)x; };
+    // size bins of the radiative transfer (code/initcld.f:141-156); the
+    // literals are REAL*4, ATHIRD = REAL*4 (1./3.)
+    const double athird = (double)(1.0f / 3.0f);
+    double rad[NBIN_RT];
+    rad[0] = R4(1.e-7);
+    rad[NBIN_RT - 1] = R4(50.e-6);
+    a.radb[0] = R4(0.0001e-6);
+    a.radb[NBIN_RT] = R4(1.e-2);
+    double vrat = std::log(rad[NBIN_RT - 1] / rad[0]) / (double)(float)(NBIN_RT - 1) * 3.0;
+    vrat = std::exp(vrat);
+    for (int i = 0; i < NBIN_RT - 1; ++i) {
+        rad[i + 1] = rad[i] * std::pow(vrat, athird);
+        a.radb[i + 1] = std::pow((2.0 * vrat) / (vrat + 1.0), athird) * rad[i];
+    }
+    std::vector<double> cv, ci, dv, di;
+    int rc = read_real4(dir + "/waterCoated_vis_JD_12bands.dat", cv, (size_t)NRATIO * NBIN_RT * 3 * NV);
+    if (!rc) rc = read_real4(dir + "/waterCoated_ir_JD_12bands.dat", ci, (size_t)NRATIO * NBIN_RT * 3 * NI);
+    if (!rc) rc = read_real4(dir + "/Dust_vis_wolff2010_JD_12bands.dat", dv, (size_t)NBIN_RT * 3 * NV);
+    if (!rc) rc = read_real4(dir + "/Dust_ir_wolff2010_JD_12bands.dat", di, (size_t)NBIN_RT * 3 * NI);
+    if (rc) return rc;
+    size_t p = 0, q = 0;
+    for (int j = 0; j < NRATIO; ++j)
+        for (int i = 0; i < NBIN_RT; ++i)
+            for (int m = 0; m < 3; ++m) {
+                for (int l = 0; l < NV; ++l) a.cld_v[m][j][i][l] = cv[p++];
+                for (int l = 0; l < NI; ++l) a.cld_i[m][j][i][l] = ci[q++];
+            }
+    p = q = 0;
+    for (int i = 0; i < NBIN_RT; ++i)
+        for (int m = 0; m < 3; ++m) {
+            for (int l = 0; l < NV; ++l) a.dst_v[m][i][l] = dv[p++];
+            for (int l = 0; l < NI; ++l) a.dst_i[m][i][l] = di[q++];
+        }
+    const float cr[NRATIO] = {0.1f, 0.2f, 0.25f, 0.3f, 0.35f, 0.4f, 0.45f, 0.5f,
+                              0.55f, 0.6f, 0.65f, 0.7f, 0.8f, 0.9f, 0.99f};
+    for (int j = 0; j < NRATIO; ++j) a.cor_ratio[j] = (double)cr[j];
+    // prescribed dust band properties (code/setrad.f90:73-105,132-155)
+    const double qev1[NV] = {1.834, 2.296, 2.672, 2.829, 2.698, 2.452, 2.261};
+    const double qsv1[NV] = {1.695, 2.031, 2.583, 2.744, 2.626, 2.225, 1.525};
+    const double gv1[NV] = {0.551, 0.640, 0.661, 0.678, 0.690, 0.743, 0.868};
+    const double qei1[NI] = {0.008, 0.262, 0.491, 1.017, 0.444};
+    const double qsi1[NI] = {0.001, 0.037, 0.122, 0.351, 0.336};
+    const double gi1[NI] = {0.004, 0.030, 0.095, 0.214, 0.316};
+    for (int n = 0; n < NV; ++n) {
+        a.qextv[n] = qev1[n];
+        a.qscatv[n] = qsv1[n] >= qev1[n] ? R4(0.99999) * qev1[n] : qsv1[n];
+        a.gv[n] = gv1[n];
+    }
+    for (int n = 0; n < NI; ++n) {
+        a.qexti[n] = qei1[n];
+        a.qscati[n] = qsi1[n] >= qei1[n] ? R4(0.99999) * qei1[n] : qsi1[n];
+        a.gi[n] = gi1[n];
+    }
     return 0;
 }
 

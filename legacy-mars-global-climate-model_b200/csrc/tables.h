@@ -32,6 +32,22 @@ void build_tables(HostTables &t, const std::vector<double> &co2v8, const double 
 
 int load_tables(const std::string &dir, HostTables &t);
 
+// Aerosol optics tables (code/initcld.f:141-190, code/setrad.f90:73-105).
+constexpr int NBIN_RT = 20, NRATIO = 15;
+struct AerosolTables {
+    double radb[NBIN_RT + 1];                 // radb_rt: bin boundaries (m)
+    // Mie tables (REAL*4 in the reference), [quantity qext,qscat,g][bin][band]
+    double dst_v[3][NBIN_RT][NV], dst_i[3][NBIN_RT][NI];
+    // water-ice coated spheres, [quantity][core ratio][bin][band]
+    double cld_v[3][NRATIO][NBIN_RT][NV], cld_i[3][NRATIO][NBIN_RT][NI];
+    double cor_ratio[NRATIO];                 // REAL*4 core-to-mantle radius ratios
+    // prescribed dust (ini_optdst via setrad): per-band QEXT, QSCAT, G
+    double qextv[NV], qscatv[NV], gv[NV], qexti[NI], qscati[NI], gi[NI];
+};
+
+// Reads the dust and water-ice Mie tables and builds the bins.  0 or <0.
+int load_aerosol_tables(const std::string &dir, AerosolTables &a);
+
 // Device k-table layout: [nw][nt][np][nh][ng 0..15], Gauss point fastest.
 void gauss_fastest(const HostTables &t, std::vector<double> &kv, std::vector<double> &ki);
 

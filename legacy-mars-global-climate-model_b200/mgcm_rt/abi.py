@@ -27,7 +27,10 @@ _D = C.POINTER(C.c_double)
 
 class Config(C.Structure):
     _fields_ = [("max_layers", C.c_int), ("precision", C.c_int), ("device", C.c_int),
-                ("validate", C.c_int), ("hbm_budget", C.c_size_t)]
+                ("validate", C.c_int), ("hbm_budget", C.c_size_t), ("solver", C.c_int)]
+
+
+SOLVER_AUTO, SOLVER_THREAD, SOLVER_QUAD = 0, 1, 2
 
 
 _IN_PTRS = ("sigma", "sol", "plev", "tlev", "pmid", "tmid", "qh2o", "tauref", "qextrefdst",
@@ -57,6 +60,15 @@ class RTError(RuntimeError):
     def __init__(self, code: int, where: str):
         self.code = code
         super().__init__(f"{where}: {STATUS.get(code, code)} ({lib().mgcm_rt_strerror(code).decode()})")
+
+
+_TR_PTRS = ("sigma", "sol", "plev", "tlev", "pmid", "tmid", "qh2o", "tauref", "dust_mass", "dust_number",
+            "ice_mass", "ice_core_mass", "ice_number", "acosz", "als", "albi", "pcol", "detau", "cumtauv")
+
+
+class BatchTracers(C.Structure):
+    _fields_ = [("ncol", C.c_int), ("nlayers", C.c_int), ("device_ptrs", C.c_int), ("active_dust", C.c_int),
+                ("cloudon", C.c_int), ("ptrop", C.c_double)] + [(n, C.c_void_p) for n in _TR_PTRS]
 
 
 class Tune(C.Structure):
@@ -93,6 +105,7 @@ def lib():
         L.mgcm_rt_strerror.restype = C.c_char_p
         L.mgcm_rt_strerror.argtypes = [C.c_int]
         L.mgcm_rt_version.restype = C.c_char_p
+        L.mgcm_rt_run_tracers.argtypes = [C.c_void_p, C.POINTER(BatchTracers), C.POINTER(BatchOut)]
         L.mgcm_rt_graph_create.argtypes = [C.c_void_p, C.c_int, C.POINTER(BatchIn), C.POINTER(BatchOut),
                                            C.c_int, C.POINTER(C.c_void_p)]
         L.mgcm_rt_graph_launch.argtypes = [C.c_void_p, C.c_void_p]
@@ -159,8 +172,8 @@ class Radiation:
     """A handle on one GPU: tables resident in HBM, runs batches of columns."""
 
     def __init__(self, data_dir, max_layers: int = 48, precision: int = FP64, device: int = 0,
-                 validate: bool = True, hbm_budget: int = 0):
-        cfg = Config(max_layers, precision, device, 1 if validate else 0, hbm_budget)
+                 validate: bool = True, hbm_budget: int = 0, solver: int = 0):
+        cfg = Config(max_layers, precision, device, 1 if validate else 0, hbm_budget, solver)
         st = C.c_int(0)
         self._h = lib().mgcm_rt_create(C.byref(cfg), str(data_dir).encode(), C.byref(st))
         if not self._h:
@@ -255,6 +268,39 @@ class Radiation:
             o["detau"] = b["detau"]
             o["cumtauv"] = b["cumtauv"]
         return outs
+
+    # ---- tracer inputs (aerosol optics on the device) -----------------
+    def run_tracers(self, t: dict, out: dict | None = None, inplace: bool = False) -> dict:
+        """Radiation from tracer mixing ratios (synth.make_tracer_batch layout):
+        the device fills the per-level dust/ice optical properties, then runs
+        the radiation.  Host or CUDA inputs as in run()."""
+        dev = _is_torch(t["plev"]) and t["plev"].is_cuda
+        if not dev and not inplace:
+            t = dict(t)
+            t["detau"] = np.array(t["detau"], dtype=np.float64, copy=True)
+            t["cumtauv"] = np.array(t["cumtauv"], dtype=np.float64, copy=True)
+        keep: list = []
+        s = BatchTracers()
+        s.ncol, s.nlayers = int(t["ncol"]), int(t["L"])
+        s.device_ptrs = 1 if dev else 0
+        s.active_dust = 1 if t.get("active_dust", 0) else 0
+        s.cloudon = 1 if t.get("cloudon", 0) else 0
+        s.ptrop = float(t["ptrop"])
+        for n in _TR_PTRS:
+            a = t.get(n)
+            if a is not None and not dev:
+                a = _host(a)
+            if a is not None:
+                keep.append(a)
+            setattr(s, n, _ptr(a))
+        if out is None:
+            out = alloc_outputs(s.ncol, s.nlayers, device=t["plev"].device if dev else None)
+        bo = make_out(out)
+        rc = lib().mgcm_rt_run_tracers(self._h, C.byref(s), C.byref(bo))
+        if rc != 0:
+            raise RTError(rc, "mgcm_rt_run_tracers")
+        out["detau"], out["cumtauv"] = t["detau"], t["cumtauv"]
+        return out
 
     # ---- captured uneven batches --------------------------------------
     def graph(self, batches: list, outs: list | None = None, autotune: bool = True) -> "Graph":

@@ -343,3 +343,65 @@ def _ice_clouds(rng, ncol, L, pl, data_dir):
     return (dict(taurefcld=tauc, qextrefcld=qextref, qxvcld=qxv, qsvcld=qsv, gvcld=gv,
                  qxicld=qxi, qsicld=qsi, gicld=gi),
             "tables" if tab is not None else "fixed-properties")
+
+
+def make_tracer_batch(ncol: int, L: int = 24, seed: int = 0, active_dust: bool = True,
+                      cloudon: bool = True, night_frac: float = 0.5, data_dir=None):
+    """Inputs of mgcm_rt_run_tracers: the column state of make_batch (dust
+    off, its Conrath TAUREF kept for prescribed dust) plus per-layer tracer
+    mixing ratios as COMP3's QTRACE holds them (code/comp3.f:592-630):
+      dust  mass Ma [kg/kg] and number Nb [1/kg] sized so that OPT_DST gives
+            roughly the Conrath profile's optical depth (effective radius
+            U[0.8, 2.0] um per column); layers of negligible dust fall below
+            OPT_DST's thresholds;
+      ice   1-3 contiguous layers with ice mass, core (dust) mass and number
+            (radius U[1, 5] um, optical depth lognormal(0.05, 1), core mass
+            fraction U[0, 0.5])."""
+    b = make_batch(ncol, L=L, seed=seed, cloud=False, night_frac=night_frac, data_dir=data_dir)
+    rng = np.random.default_rng(seed + 7919)
+    lev = 2 * L + 3
+    pl = b["plev"]
+    mass = np.empty((ncol, L))   # kg/m^2 of the layer's first radiation level pair
+    for l in range(1, L + 1):
+        k = 2 * l + 2
+        mass[:, l - 1] = 100.0 * (pl[:, k - 1] - pl[:, k - 3]) / GRAV
+    t = {k: v for k, v in b.items() if k not in (
+        "qextrefdst", "qxvdst", "qsvdst", "gvdst", "qxidst", "qsidst", "gidst")}
+    t["active_dust"] = 1 if active_dust else 0
+    t["cloudon"] = 1 if cloudon else 0
+    if active_dust:
+        r = rng.uniform(0.8e-6, 2.0e-6, ncol)[:, None]
+        tau = np.empty((ncol, L))
+        for l in range(1, L + 1):
+            tau[:, l - 1] = b["tauref"][:, 2 * l + 1] + b["tauref"][:, 2 * l + 2]
+        no = tau / (math.pi * r * r * 2.5 * np.maximum(mass, 1e-12))
+        ma = no * (4.0 / 3.0) * math.pi * r ** 3 * 2500.0
+        t["dust_number"] = no
+        t["dust_mass"] = ma
+    else:
+        t["dust_number"] = None
+        t["dust_mass"] = None
+    if cloudon:
+        ima = np.zeros((ncol, L))
+        icor = np.zeros((ncol, L))
+        inb = np.zeros((ncol, L))
+        tau_ice = 0.05 * np.exp(rng.standard_normal(ncol))
+        nlay = rng.integers(1, 4, ncol)
+        start = rng.integers(max(1, L // 3), max(2, L - 3), ncol)
+        r = rng.uniform(1.0e-6, 5.0e-6, ncol)
+        fcor = rng.uniform(0.0, 0.5, ncol)
+        for j in range(3):
+            on = j < nlay
+            l = np.minimum(start + j, L)
+            c = np.arange(ncol)[on]
+            m = mass[c, l[on] - 1]
+            n = tau_ice[on] / nlay[on] / (math.pi * r[on] ** 2 * 2.0 * np.maximum(m, 1e-12))
+            mtot = n * (4.0 / 3.0) * math.pi * r[on] ** 3 * 917.0
+            inb[c, l[on] - 1] = n
+            icor[c, l[on] - 1] = fcor[on] * mtot
+            ima[c, l[on] - 1] = (1.0 - fcor[on]) * mtot
+        t["ice_mass"], t["ice_core_mass"], t["ice_number"] = ima, icor, inb
+    else:
+        t["ice_mass"] = t["ice_core_mass"] = t["ice_number"] = None
+    t["meta"] = dict(b["meta"], tracers=True)
+    return t

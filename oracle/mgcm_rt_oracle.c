@@ -66,6 +66,7 @@ static const double WREFH2O_TAB[ORC_REFH2O] = {1.0e-7, 1.0e-6, 1.0e-5, 1.0e-4, 1
                                                1.0e-2, 1.0e-1, 2.0e-1, 3.0e-1, 4.0e-1};
 
 size_t orc_tables_size(void) { return sizeof(orc_tables); }
+size_t orc_aero_size(void) { return sizeof(orc_aero); }
 
 /* ------------------------------------------------------------------ */
 /* Set-up                                                               */
@@ -1184,3 +1185,234 @@ void orc_dsolflux(const orc_tables *t, int ncol, const double *sol, const double
 /* The column exponential and logarithm, exported for tests. */
 double orc_exp(double x) { return cexp_(x); }
 double orc_log10(double x) { return mgcm_rt_log10(x); }
+double orc_erf(double x) { return mgcm_rt_erf(x); }
+double orc_ln(double x) { return mgcm_rt_ln(x); }
+double orc_pow(double x, double y) { return mgcm_rt_pow(x, y); }
+
+/* ======================================================================
+ * Aerosol optics.  Table set-up: code/initcld.f:141-190 (bins, REAL*4
+ * literals, ATHIRD = REAL*4 (1./3.)), code/setrad.f90:73-105,132-155.
+ * Per column: code/opt_dst.f:55-161, code/opt_cld.f:55-188,
+ * code/ini_optdst.f:29-51, the choice in code/comp3.f:592-630.  Powers,
+ * logs, exps and DERF use the deterministic routines of mgcm_rt_math.h. */
+static int read_real4(const char *path, double *v, size_t n) {
+    FILE *f = fopen(path, "r");
+    if (!f) return -1;
+    size_t k = 0;
+    char tok[64];
+    while (k < n && fscanf(f, "%63s", tok) == 1) v[k++] = (double)strtof(tok, NULL);
+    fclose(f);
+    return k == n ? 0 : -2;
+}
+
+int orc_aero_load(orc_aero *a, const char *dir) {
+    const double athird = (double)(1.0f / 3.0f);
+    double rad[ORC_NBIN];
+    rad[0] = R4(1.e-7);
+    rad[ORC_NBIN - 1] = R4(50.e-6);
+    a->radb[0] = R4(0.0001e-6);
+    a->radb[ORC_NBIN] = R4(1.e-2);
+    double vrat = log(rad[ORC_NBIN - 1] / rad[0]) / (double)(float)(ORC_NBIN - 1) * 3.0;
+    vrat = exp(vrat);
+    for (int i = 0; i < ORC_NBIN - 1; ++i) {
+        rad[i + 1] = rad[i] * pow(vrat, athird);
+        a->radb[i + 1] = pow((2.0 * vrat) / (vrat + 1.0), athird) * rad[i];
+    }
+    const size_t ncv = (size_t)ORC_NRATIO * ORC_NBIN * 3 * ORC_NSPECTV, nci = (size_t)ORC_NRATIO * ORC_NBIN * 3 * ORC_NSPECTI;
+    const size_t ndv = (size_t)ORC_NBIN * 3 * ORC_NSPECTV, ndi = (size_t)ORC_NBIN * 3 * ORC_NSPECTI;
+    double *cv = malloc(ncv * 8), *ci = malloc(nci * 8), *dv = malloc(ndv * 8), *di = malloc(ndi * 8);
+    char path[4096];
+    int rc = 0;
+    snprintf(path, sizeof path, "%s/waterCoated_vis_JD_12bands.dat", dir);
+    rc = rc ? rc : read_real4(path, cv, ncv);
+    snprintf(path, sizeof path, "%s/waterCoated_ir_JD_12bands.dat", dir);
+    rc = rc ? rc : read_real4(path, ci, nci);
+    snprintf(path, sizeof path, "%s/Dust_vis_wolff2010_JD_12bands.dat", dir);
+    rc = rc ? rc : read_real4(path, dv, ndv);
+    snprintf(path, sizeof path, "%s/Dust_ir_wolff2010_JD_12bands.dat", dir);
+    rc = rc ? rc : read_real4(path, di, ndi);
+    if (!rc) {
+        size_t p = 0, q = 0;
+        /* read(60) (qextv_cld(j,i,l), l=1,7) then qscatv, gv, for j, i */
+        for (int j = 0; j < ORC_NRATIO; ++j)
+            for (int i = 0; i < ORC_NBIN; ++i)
+                for (int m = 0; m < 3; ++m) {
+                    for (int l = 0; l < ORC_NSPECTV; ++l) a->cld_v[m][j][i][l] = cv[p++];
+                    for (int l = 0; l < ORC_NSPECTI; ++l) a->cld_i[m][j][i][l] = ci[q++];
+                }
+        p = q = 0;
+        for (int i = 0; i < ORC_NBIN; ++i)
+            for (int m = 0; m < 3; ++m) {
+                for (int l = 0; l < ORC_NSPECTV; ++l) a->dst_v[m][i][l] = dv[p++];
+                for (int l = 0; l < ORC_NSPECTI; ++l) a->dst_i[m][i][l] = di[q++];
+            }
+    }
+    free(cv);
+    free(ci);
+    free(dv);
+    free(di);
+    if (rc) return rc;
+    static const float cr[ORC_NRATIO] = {0.1f, 0.2f, 0.25f, 0.3f, 0.35f, 0.4f, 0.45f, 0.5f,
+                                         0.55f, 0.6f, 0.65f, 0.7f, 0.8f, 0.9f, 0.99f};
+    memcpy(a->cor_ratio, cr, sizeof cr);
+    static const double qev1[7] = {1.834, 2.296, 2.672, 2.829, 2.698, 2.452, 2.261};
+    static const double qsv1[7] = {1.695, 2.031, 2.583, 2.744, 2.626, 2.225, 1.525};
+    static const double gv1[7] = {0.551, 0.640, 0.661, 0.678, 0.690, 0.743, 0.868};
+    static const double qei1[5] = {0.008, 0.262, 0.491, 1.017, 0.444};
+    static const double qsi1[5] = {0.001, 0.037, 0.122, 0.351, 0.336};
+    static const double gi1[5] = {0.004, 0.030, 0.095, 0.214, 0.316};
+    for (int n = 0; n < 7; ++n) {
+        a->qextv[n] = qev1[n];
+        a->qscatv[n] = qsv1[n] >= qev1[n] ? R4(0.99999) * qev1[n] : qsv1[n];
+        a->gv[n] = gv1[n];
+    }
+    for (int n = 0; n < 5; ++n) {
+        a->qexti[n] = qei1[n];
+        a->qscati[n] = qsi1[n] >= qei1[n] ? R4(0.99999) * qei1[n] : qsi1[n];
+        a->gi[n] = gi1[n];
+    }
+    return 0;
+}
+
+/* One column of OPT_DST (cld = 0) or OPT_CLD (cld = 1). */
+static void opt_aerosol(const orc_aero *a, int cld, int L, const double *pl, const double *ma,
+                        const double *mcor, const double *nb, double *tauref, double *qextref,
+                        double *qxv, double *qsv, double *gv, double *qxi, double *qsi, double *gi) {
+    const int lev1 = 2 * L + 4;
+    const double PIc = 3.1415926535897932, GRAVc = 3.72;
+    const double athird = (double)(1.0f / 3.0f);
+    const double dpden_dt = R4(2.5E+3), dpden_ice = R4(917.);
+    for (int k = 0; k < lev1; ++k) {
+        qextref[k] = 1.0;
+        tauref[k] = 0.0;
+    }
+    for (int i = 0; i < ORC_NSPECTV; ++i)
+        for (int k = 0; k < lev1; ++k) {
+            qxv[i * lev1 + k] = qextref[k];
+            qsv[i * lev1 + k] = qextref[k] * R4(0.99);
+            gv[i * lev1 + k] = 0.0;
+        }
+    for (int i = 0; i < ORC_NSPECTI; ++i)
+        for (int k = 0; k < lev1; ++k) {
+            qxi[i * lev1 + k] = qextref[k];
+            qsi[i * lev1 + k] = qextref[k] * R4(0.99);
+            gi[i * lev1 + k] = 0.0;
+        }
+    const double dev = cld ? R4(0.3087) : R4(0.63676);
+    const double dev2 = 1.0 / ((double)sqrtf(2.0f) * dev);
+    for (int l = 1; l <= L; ++l) {
+        double Mo, No, dens;
+        int irap = ORC_NRATIO;
+        if (!cld) {
+            if (!(ma[l - 1] > R4(1.e-8) && nb[l - 1] > 1.0)) continue;
+            Mo = ma[l - 1];
+            No = nb[l - 1] + 1.0;
+            dens = dpden_dt;
+        } else {
+            if (!(ma[l - 1] + mcor[l - 1] > R4(1.e-7) && nb[l - 1] > 1.0)) continue;
+            float mtc = (float)(mcor[l - 1] / dpden_dt / (ma[l - 1] / dpden_ice + mcor[l - 1] / dpden_dt));
+            mtc = (float)mgcm_rt_pow((double)mtc, athird);
+            for (int i = 1; i <= ORC_NRATIO; ++i) {
+                if (mtc < a->cor_ratio[i - 1] && i != 1) {
+                    irap = i - 1;
+                    break;
+                } else if (mtc == a->cor_ratio[i - 1]) {
+                    irap = i;
+                    break;
+                } else if (mtc < a->cor_ratio[i - 1] && i == 1) {
+                    irap = 1;
+                    break;
+                }
+            }
+            Mo = ma[l - 1] + mcor[l - 1];
+            No = nb[l - 1];
+            dens = ma[l - 1] / Mo * dpden_ice + mcor[l - 1] / Mo * dpden_dt;
+        }
+        const double cst = 0.75 / (PIc * dens);
+        double Rs = mgcm_rt_pow(Mo / No * cst, athird) * mgcm_rt_exp(-0.5 * (dev * dev));
+        const double Ao = No * PIc * (Rs * Rs);
+        Rs = Rs * mgcm_rt_exp(1.5 * (dev * dev));
+        const double rmax = cld ? R4(100.e-6) : R4(50.e-6);
+        Rs = fmin(fmax(Rs, R4(1.e-7)), rmax);
+        Rs = 1.0 / Rs;
+        double surf[ORC_NBIN];
+        for (int i = 0; i < ORC_NBIN; ++i)
+            surf[i] = 0.5 * (mgcm_rt_erf(mgcm_rt_ln(a->radb[i + 1] * Rs) * dev2) -
+                             mgcm_rt_erf(mgcm_rt_ln(a->radb[i] * Rs) * dev2));
+        for (int nn = 1; nn <= 2; ++nn) {
+            const int k = 2 * l + 1 + nn; /* 1-based */
+            for (int iw = 0; iw < ORC_NSPECTV; ++iw) {
+                double x = 0.0, sc = 0.0, g = gv[iw * lev1 + k - 1];
+                for (int i = 0; i < ORC_NBIN; ++i) {
+                    const double qe = cld ? a->cld_v[0][irap - 1][i][iw] : a->dst_v[0][i][iw];
+                    const double qs = cld ? a->cld_v[1][irap - 1][i][iw] : a->dst_v[1][i][iw];
+                    const double qg = cld ? a->cld_v[2][irap - 1][i][iw] : a->dst_v[2][i][iw];
+                    x = x + surf[i] * qe;
+                    sc = sc + surf[i] * qs;
+                    g = g + surf[i] * qg;
+                }
+                qxv[iw * lev1 + k - 1] = x;
+                qsv[iw * lev1 + k - 1] = fmin(sc, R4(0.99999) * x);
+                gv[iw * lev1 + k - 1] = g;
+            }
+            for (int iw = 0; iw < ORC_NSPECTI; ++iw) {
+                double x = 0.0, sc = 0.0, g = gi[iw * lev1 + k - 1];
+                for (int i = 0; i < ORC_NBIN; ++i) {
+                    const double qe = cld ? a->cld_i[0][irap - 1][i][iw] : a->dst_i[0][i][iw];
+                    const double qs = cld ? a->cld_i[1][irap - 1][i][iw] : a->dst_i[1][i][iw];
+                    const double qg = cld ? a->cld_i[2][irap - 1][i][iw] : a->dst_i[2][i][iw];
+                    x = x + surf[i] * qe;
+                    sc = sc + surf[i] * qs;
+                    g = g + surf[i] * qg;
+                }
+                qxi[iw * lev1 + k - 1] = x;
+                qsi[iw * lev1 + k - 1] = fmin(sc, R4(0.99999) * x);
+                gi[iw * lev1 + k - 1] = g;
+            }
+            qextref[k - 1] = qxv[5 * lev1 + k - 1]; /* L_NREFV = 6 */
+            const double mass = 100.0 * (pl[k - 1] - pl[k - 2]) / GRAVc;
+            tauref[k - 1] = Ao * qextref[k - 1] * mass;
+        }
+    }
+}
+
+void orc_aerosols(const orc_aero *a, const orc_tracers *t) {
+    const int L = t->L, lev = 2 * L + 3, lev1 = lev + 1;
+    for (int c = 0; c < t->ncol; ++c) {
+        const double *pl = t->plev + (size_t)c * lev;
+        double *tr = t->tauref + (size_t)c * lev1, *qr = t->qextrefdst + (size_t)c * lev1;
+        double *xv = t->qxvdst + (size_t)c * 7 * lev1, *sv = t->qsvdst + (size_t)c * 7 * lev1;
+        double *gv = t->gvdst + (size_t)c * 7 * lev1, *xi = t->qxidst + (size_t)c * 5 * lev1;
+        double *si = t->qsidst + (size_t)c * 5 * lev1, *gi = t->gidst + (size_t)c * 5 * lev1;
+        if (t->active_dust) {
+            opt_aerosol(a, 0, L, pl, t->dust_mass + (size_t)c * L, NULL, t->dust_number + (size_t)c * L,
+                        tr, qr, xv, sv, gv, xi, si, gi);
+            for (int k = 0; k < 3; ++k) tr[k] = 0.0; /* code/comp3.f:602-605 */
+        } else { /* code/ini_optdst.f:29-51 with TAUREF from filltaucum */
+            for (int k = 0; k < lev1; ++k) {
+                qr[k] = a->qextv[5];
+                tr[k] = t->tauref_in[(size_t)c * lev1 + k];
+            }
+            for (int i = 0; i < 7; ++i)
+                for (int k = 0; k < lev1; ++k) {
+                    xv[i * lev1 + k] = a->qextv[i];
+                    sv[i * lev1 + k] = a->qscatv[i];
+                    gv[i * lev1 + k] = a->gv[i];
+                }
+            for (int i = 0; i < 5; ++i)
+                for (int k = 0; k < lev1; ++k) {
+                    xi[i * lev1 + k] = a->qexti[i];
+                    si[i * lev1 + k] = a->qscati[i];
+                    gi[i * lev1 + k] = a->gi[i];
+                }
+        }
+        tr[lev1 - 1] = 0.0; /* code/comp3.f:618 */
+        if (t->cloudon)
+            opt_aerosol(a, 1, L, pl, t->ice_mass + (size_t)c * L, t->ice_core + (size_t)c * L,
+                        t->ice_number + (size_t)c * L, t->taurefcld + (size_t)c * lev1,
+                        t->qextrefcld + (size_t)c * lev1, t->qxvcld + (size_t)c * 7 * lev1,
+                        t->qsvcld + (size_t)c * 7 * lev1, t->gvcld + (size_t)c * 7 * lev1,
+                        t->qxicld + (size_t)c * 5 * lev1, t->qsicld + (size_t)c * 5 * lev1,
+                        t->gicld + (size_t)c * 5 * lev1);
+    }
+}

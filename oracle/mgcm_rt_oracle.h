@@ -110,6 +110,37 @@ void orc_optics_column(const orc_tables *t, const orc_batch *b, int col,
                        double *taucumi, double *taugsurfi);
 
 /* dsolflux.f: direct-beam surface flux from DETAU, per column. */
+/* ---- aerosol optics (code/opt_dst.f, code/opt_cld.f, code/ini_optdst.f,
+ * code/initcld.f:141-190, code/setrad.f90:73-105, code/comp3.f:592-630) */
+#define ORC_NBIN 20
+#define ORC_NRATIO 15
+typedef struct {
+    double radb[ORC_NBIN + 1];
+    double dst_v[3][ORC_NBIN][ORC_NSPECTV], dst_i[3][ORC_NBIN][ORC_NSPECTI];
+    double cld_v[3][ORC_NRATIO][ORC_NBIN][ORC_NSPECTV], cld_i[3][ORC_NRATIO][ORC_NBIN][ORC_NSPECTI];
+    float cor_ratio[ORC_NRATIO];
+    double qextv[ORC_NSPECTV], qscatv[ORC_NSPECTV], gv[ORC_NSPECTV];
+    double qexti[ORC_NSPECTI], qscati[ORC_NSPECTI], gi[ORC_NSPECTI];
+} orc_aero;
+
+/* Reads the dust and water-ice Mie tables of `dir` and builds the size bins. */
+int orc_aero_load(orc_aero *a, const char *dir);
+size_t orc_aero_size(void);
+
+/* Tracer inputs of a batch -> the full per-level aerosol arrays of orc_batch.
+ * active_dust: opt_dst from the dust mass/number mixing ratios, else the
+ * prescribed band properties with TAUREF copied from tauref_in;
+ * cloudon: opt_cld from the ice mass, core mass and number mixing ratios.
+ * Tracers are [ncol][L] (QTRACE(J,I,L,*)); outputs as in orc_batch. */
+typedef struct {
+    int ncol, L, active_dust, cloudon;
+    const double *plev, *tauref_in;
+    const double *dust_mass, *dust_number, *ice_mass, *ice_core, *ice_number;
+    double *tauref, *qextrefdst, *qxvdst, *qsvdst, *gvdst, *qxidst, *qsidst, *gidst;
+    double *taurefcld, *qextrefcld, *qxvcld, *qsvcld, *gvcld, *qxicld, *qsicld, *gicld;
+} orc_tracers;
+void orc_aerosols(const orc_aero *a, const orc_tracers *t);
+
 void orc_dsolflux(const orc_tables *t, int ncol, const double *sol, const double *acosz,
                   const double *detau, double *directsol);
 

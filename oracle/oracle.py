@@ -183,3 +183,68 @@ def dsolflux(tables: Tables, sol, acosz, detau) -> np.ndarray:
     out = np.zeros(acosz.shape[0])
     lib(tables.variant).orc_dsolflux(tables.ptr, acosz.shape[0], _p(sol), _p(acosz), _p(detau), _p(out))
     return out
+
+
+# ---- aerosol optics (code/opt_dst.f, code/opt_cld.f, code/ini_optdst.f)
+class OrcTracers(C.Structure):
+    _fields_ = [("ncol", C.c_int), ("L", C.c_int), ("active_dust", C.c_int), ("cloudon", C.c_int)] + [
+        (n, C.c_void_p) for n in ("plev", "tauref_in", "dust_mass", "dust_number", "ice_mass", "ice_core",
+                                  "ice_number", "tauref", "qextrefdst", "qxvdst", "qsvdst", "gvdst", "qxidst",
+                                  "qsidst", "gidst", "taurefcld", "qextrefcld", "qxvcld", "qsvcld", "gvcld",
+                                  "qxicld", "qsicld", "gicld")]
+
+
+class AeroTables:
+    """Dust and water-ice Mie tables and size bins (orc_aero_load)."""
+
+    def __init__(self, data_dir, variant: str = "rt"):
+        L = lib(variant)
+        L.orc_aero_load.argtypes = [C.c_void_p, C.c_char_p]
+        L.orc_aerosols.argtypes = [C.c_void_p, C.POINTER(OrcTracers)]
+        self.variant = variant
+        L.orc_aero_size.restype = C.c_size_t
+        self._buf = C.create_string_buffer(int(L.orc_aero_size()) + 64)
+        rc = L.orc_aero_load(self._buf, str(data_dir).encode())
+        if rc != 0:
+            raise FileNotFoundError(f"aerosol tables not readable in {data_dir} ({rc})")
+        self.ptr = C.cast(self._buf, C.c_void_p)
+
+
+def aerosols(aero: AeroTables, tb: dict) -> dict:
+    """Tracer batch -> the standard batch dict (per-level aerosol arrays filled
+    as COMP3 fills them), ready for run_batch."""
+    ncol, L = int(tb["ncol"]), int(tb["L"])
+    lev1 = 2 * L + 4
+    out = {k: v for k, v in tb.items()}
+    keep = []
+    def arr(shape):
+        a = np.zeros(shape)
+        keep.append(a)
+        return a
+    names_d = ("tauref", "qextrefdst", "qxvdst", "qsvdst", "gvdst", "qxidst", "qsidst", "gidst")
+    names_c = ("taurefcld", "qextrefcld", "qxvcld", "qsvcld", "gvcld", "qxicld", "qsicld", "gicld")
+    shapes = ((ncol, lev1), (ncol, lev1), (ncol, 7, lev1), (ncol, 7, lev1), (ncol, 7, lev1),
+              (ncol, 5, lev1), (ncol, 5, lev1), (ncol, 5, lev1))
+    for n, sh in zip(names_d, shapes):
+        out[n] = arr(sh)
+    cloud = bool(tb.get("cloudon", 0))
+    for n, sh in zip(names_c, shapes):
+        out[n] = arr(sh) if cloud else None
+    s = OrcTracers()
+    s.ncol, s.L = ncol, L
+    s.active_dust = 1 if tb.get("active_dust", 0) else 0
+    s.cloudon = 1 if cloud else 0
+    src = {"plev": "plev", "tauref_in": "tauref", "dust_mass": "dust_mass", "dust_number": "dust_number",
+           "ice_mass": "ice_mass", "ice_core": "ice_core_mass", "ice_number": "ice_number"}
+    for f, k in src.items():
+        v = tb.get(k)
+        if v is not None:
+            v = np.ascontiguousarray(v, dtype=np.float64)
+            keep.append(v)
+        setattr(s, f, v.ctypes.data if v is not None else None)
+    for n in names_d + names_c:
+        setattr(s, n, out[n].ctypes.data if out[n] is not None else None)
+    lib(aero.variant).orc_aerosols(aero.ptr, C.byref(s))
+    for k in ("dust_mass", "dust_number", "ice_mass", "ice_core_mass", "ice_number", "active_dust", "cloudon"):
+        out.pop(k, None)
+    return out

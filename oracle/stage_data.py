@@ -11,7 +11,8 @@ import shutil
 import sys
 
 FILES = ("CO2H2O_V_12_95_INTEL", "CO2H2O_IR_12_95_INTEL",
-         "waterCoated_vis_JD_12bands.dat", "waterCoated_ir_JD_12bands.dat")
+         "waterCoated_vis_JD_12bands.dat", "waterCoated_ir_JD_12bands.dat",
+         "Dust_vis_wolff2010_JD_12bands.dat", "Dust_ir_wolff2010_JD_12bands.dat")
 DEFAULT_SRC = pathlib.Path("/root/reference/run/data")
 DST = pathlib.Path(__file__).resolve().parents[1] / "data"
 
