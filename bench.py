@@ -6,15 +6,23 @@ the reference's input recipe (mgcm_rt.synth), real k tables when staged.
 Inputs (2.5 GB) are larger than L2 (126 MB), so no flush is needed between steps.
 
   value  columns/s with inputs resident in HBM (device pointers, C ABI
-         mgcm_rt_enqueue), CUDA events on the launching stream, max over ranks
-  e2e    the same through mgcm_rt_run with pinned HOST buffers: every step
-         copies the batch in and the outputs back inside the timed region
+         mgcm_rt_enqueue), CUDA events on the launching stream, max over ranks;
+         the MIXED path, with FP64 timed beside it (--precision both)
+  e2e    the same workload end to end through mgcm_rt_run_tracers with pinned
+         HOST buffers (tracer inputs, aerosol optics on the device): every
+         step copies the inputs in and the outputs back inside the timed
+         region; e2e.arrays_path is the drop-in mgcm_rt_run with the per-level
+         aerosol arrays copied from the host
+  serving  p50/p99 request latency of a Poisson request stream (submit/poll)
+Workload c2 (--workload c2): 64 ensemble members on three grids in one
+captured CUDA graph.
 Multi-GPU: columns shard across ranks with no collective on the data path
 (weak scaling: each rank runs its own 64,800-column batch).
 
 --impl reference times the reference algorithm on the host cores (the FP64
-CPU oracle, a restatement of the reference Fortran, since the reference
-cannot be compiled here: no Fortran compiler) on a bounded sample per step.
+CPU oracle -- aerosol optics and radiation, a restatement of the reference
+Fortran, since the reference cannot be compiled here: no Fortran compiler)
+on a bounded sample per step.
 """
 from __future__ import annotations
 
@@ -138,27 +146,39 @@ class Clocks:
                 "samples": len(rows)}
 
 
-def cpu_baseline(batch, data_dir, budget_s=10.0):
+def _oracle_call(t, a, tb, cores):
+    """One reference-equivalent call: the aerosol optics of COMP3 and the
+    radiation (oracle restatements), both on all host cores."""
+    import oracle
+    return oracle.run_batch(t, oracle.aerosols(a, tb, cores), cores)
+
+
+def cpu_baseline(batch, data_dir, budget_s=10.0, tracers=None):
     """Oracle (FP64 restatement of the reference) on all host cores over a
-    bounded sample of the workload's columns."""
+    bounded sample of the workload's columns (tracer form: aerosol optics
+    included)."""
     import oracle
     t = oracle.Tables(data_dir)
+    a = oracle.AeroTables(data_dir) if tracers is not None else None
+    src = tracers if tracers is not None else batch
     cores = os.cpu_count() or 1
     def sub(n):
         s = {k: (v[:n] if isinstance(v, np.ndarray) and v.ndim >= 1 and k not in ("sigma", "sol") else v)
-             for k, v in batch.items()}
+             for k, v in src.items()}
         s["ncol"] = n
         return s
-    n0 = min(int(batch["ncol"]), 64 * cores)
+    run = (lambda b: _oracle_call(t, a, b, cores)) if a is not None else (lambda b: oracle.run_batch(t, b, cores))
+    n0 = min(int(src["ncol"]), 64 * cores)
     t0 = time.perf_counter()
-    oracle.run_batch(t, sub(n0), cores)
+    run(sub(n0))
     per = (time.perf_counter() - t0) / n0
-    n = int(min(batch["ncol"], max(n0, budget_s / max(per, 1e-9))))
+    n = int(min(src["ncol"], max(n0, budget_s / max(per, 1e-9))))
     t0 = time.perf_counter()
-    oracle.run_batch(t, sub(n), cores)
+    run(sub(n))
     dt = time.perf_counter() - t0
+    what = "aerosol optics + radiation" if a is not None else "radiation"
     return {"value": n / dt, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"first {n} columns of the workload, {dt:.1f} s on {cores} threads"}
+            "sample": f"first {n} columns of the workload ({what}), {dt:.1f} s on {cores} threads"}
 
 
 def run_reference(args, wl):
@@ -171,13 +191,14 @@ def run_reference(args, wl):
     t = oracle.Tables(d)
     cores = os.cpu_count() or 1
     sample = min(wl["ncol"], 16 * cores)
-    b = synth.make_batch(sample, L=wl["L"], seed=1000, cloud=wl["cloud"])
+    a = oracle.AeroTables(d)
+    b = synth.make_tracer_batch(sample, L=wl["L"], seed=1000, active_dust=False, cloudon=wl["cloud"])
     for _ in range(args.warmup):
-        oracle.run_batch(t, b, cores)
+        _oracle_call(t, a, b, cores)
     times = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        oracle.run_batch(t, b, cores)
+        _oracle_call(t, a, b, cores)
         times.append(time.perf_counter() - t0)
     v = sample * len(times) / sum(times)
     line = {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
@@ -187,7 +208,7 @@ def run_reference(args, wl):
             "config": {"workload": wl["name"], "columns": wl["ncol"], "layers": wl["L"],
                        "k_tables": kind},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
-                             "sample": f"{sample} columns per step, {cores} threads"},
+                             "sample": f"{sample} columns per step (aerosol optics + radiation), {cores} threads"},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -476,7 +497,7 @@ def main():
     rt = handles[hp]
 
     # ---- end to end through the C ABI with pinned host buffers (e2e)
-    e2e = None
+    e2e, tb = None, None
     if not args.no_e2e:
         hb, keep = {}, []
         for k, v in b.items():
@@ -503,9 +524,35 @@ def main():
         e1.record(stream)
         barrier()
         ems = max_over_ranks(e0.elapsed_time(e1) / args.steps)
-        e2e = {"value": ncol * world / (ems / 1e3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
-               "d2h_bytes_per_step": int(d2h), "ms_per_step": ems,
-               "path": f"mgcm_rt_run ({hp}), pinned host buffers"}
+        e2e_arrays = {"value": ncol * world / (ems / 1e3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                      "d2h_bytes_per_step": int(d2h), "ms_per_step": ems,
+                      "path": f"mgcm_rt_run ({hp}): per-level aerosol arrays from the host"}
+        # the same workload through mgcm_rt_run_tracers: prescribed (Conrath)
+        # dust and ice tracers; aerosol optics on the device
+        tb = synth.make_tracer_batch(ncol, L=L, seed=1000 + rank, active_dust=False, cloudon=wl["cloud"])
+        ht = {}
+        for k, v in tb.items():
+            if isinstance(v, np.ndarray):
+                tpin = torch.empty(v.shape, dtype=torch.float64, pin_memory=True)
+                tpin.numpy()[...] = v
+                keep.append(tpin)
+                ht[k] = tpin.numpy()
+            else:
+                ht[k] = v
+        h2d_t = sum(v.nbytes for v in ht.values() if isinstance(v, np.ndarray))
+        for _ in range(args.warmup):
+            rt.run_tracers(ht, ho, inplace=True)
+        barrier()
+        e0.record(stream)
+        for _ in range(args.steps):
+            rt.run_tracers(ht, ho, inplace=True)
+        e1.record(stream)
+        barrier()
+        tms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+        e2e = {"value": ncol * world / (tms / 1e3), "unit": UNIT, "h2d_bytes_per_step": int(h2d_t),
+               "d2h_bytes_per_step": int(d2h), "ms_per_step": tms,
+               "path": f"mgcm_rt_run_tracers ({hp}): tracer inputs, aerosol optics on the device",
+               "arrays_path": e2e_arrays}
 
     acc = None
     if "fp64" in outs and "mixed" in outs:
@@ -551,7 +598,7 @@ def main():
         if e2e:
             line["e2e"] = e2e
         if not args.no_cpu_baseline and world == 1:
-            line["cpu_baseline"] = cpu_baseline(b, d)
+            line["cpu_baseline"] = cpu_baseline(b, d, tracers=tb if e2e else None)
         print(json.dumps(line), flush=True)
     for h in handles.values():
         h.set_stream(None)

@@ -1376,9 +1376,44 @@ static void opt_aerosol(const orc_aero *a, int cld, int L, const double *pl, con
     }
 }
 
-void orc_aerosols(const orc_aero *a, const orc_tracers *t) {
+static void aerosols_range(const orc_aero *a, const orc_tracers *t, int c0, int c1);
+
+typedef struct {
+    const orc_aero *a;
+    const orc_tracers *t;
+    int c0, c1;
+} aero_job;
+
+static void *aero_thread(void *p) {
+    const aero_job *j = (const aero_job *)p;
+    aerosols_range(j->a, j->t, j->c0, j->c1);
+    return NULL;
+}
+
+void orc_aerosols_mt(const orc_aero *a, const orc_tracers *t, int nthreads) {
+    if (nthreads <= 0) nthreads = (int)sysconf(_SC_NPROCESSORS_ONLN);
+    if (nthreads > 256) nthreads = 256;
+    if (nthreads <= 1 || t->ncol < 2 * nthreads) {
+        aerosols_range(a, t, 0, t->ncol);
+        return;
+    }
+    pthread_t th[256];
+    aero_job jobs[256];
+    for (int i = 0; i < nthreads; ++i) {
+        jobs[i].a = a;
+        jobs[i].t = t;
+        jobs[i].c0 = (int)((long long)t->ncol * i / nthreads);
+        jobs[i].c1 = (int)((long long)t->ncol * (i + 1) / nthreads);
+        pthread_create(&th[i], NULL, aero_thread, &jobs[i]);
+    }
+    for (int i = 0; i < nthreads; ++i) pthread_join(th[i], NULL);
+}
+
+void orc_aerosols(const orc_aero *a, const orc_tracers *t) { aerosols_range(a, t, 0, t->ncol); }
+
+static void aerosols_range(const orc_aero *a, const orc_tracers *t, int c0, int c1) {
     const int L = t->L, lev = 2 * L + 3, lev1 = lev + 1;
-    for (int c = 0; c < t->ncol; ++c) {
+    for (int c = c0; c < c1; ++c) {
         const double *pl = t->plev + (size_t)c * lev;
         double *tr = t->tauref + (size_t)c * lev1, *qr = t->qextrefdst + (size_t)c * lev1;
         double *xv = t->qxvdst + (size_t)c * 7 * lev1, *sv = t->qsvdst + (size_t)c * 7 * lev1;

@@ -140,6 +140,8 @@ typedef struct {
     double *taurefcld, *qextrefcld, *qxvcld, *qsvcld, *gvcld, *qxicld, *qsicld, *gicld;
 } orc_tracers;
 void orc_aerosols(const orc_aero *a, const orc_tracers *t);
+/* The same over nthreads host threads (<= 0: all). */
+void orc_aerosols_mt(const orc_aero *a, const orc_tracers *t, int nthreads);
 
 void orc_dsolflux(const orc_tables *t, int ncol, const double *sol, const double *acosz,
                   const double *detau, double *directsol);

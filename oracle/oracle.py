@@ -201,6 +201,7 @@ class AeroTables:
         L = lib(variant)
         L.orc_aero_load.argtypes = [C.c_void_p, C.c_char_p]
         L.orc_aerosols.argtypes = [C.c_void_p, C.POINTER(OrcTracers)]
+        L.orc_aerosols_mt.argtypes = [C.c_void_p, C.POINTER(OrcTracers), C.c_int]
         self.variant = variant
         L.orc_aero_size.restype = C.c_size_t
         self._buf = C.create_string_buffer(int(L.orc_aero_size()) + 64)
@@ -210,7 +211,7 @@ class AeroTables:
         self.ptr = C.cast(self._buf, C.c_void_p)
 
 
-def aerosols(aero: AeroTables, tb: dict) -> dict:
+def aerosols(aero: AeroTables, tb: dict, nthreads: int = 1) -> dict:
     """Tracer batch -> the standard batch dict (per-level aerosol arrays filled
     as COMP3 fills them), ready for run_batch."""
     ncol, L = int(tb["ncol"]), int(tb["L"])
@@ -244,7 +245,7 @@ def aerosols(aero: AeroTables, tb: dict) -> dict:
         setattr(s, f, v.ctypes.data if v is not None else None)
     for n in names_d + names_c:
         setattr(s, n, out[n].ctypes.data if out[n] is not None else None)
-    lib(aero.variant).orc_aerosols(aero.ptr, C.byref(s))
+    lib(aero.variant).orc_aerosols_mt(aero.ptr, C.byref(s), nthreads)
     for k in ("dust_mass", "dust_number", "ice_mass", "ice_core_mass", "ice_number", "active_dust", "cloudon"):
         out.pop(k, None)
     return out
