@@ -17,7 +17,8 @@ Inputs (2.5 GB) are larger than L2 (126 MB), so no flush is needed between steps
 Workload c2 (--workload c2): 64 ensemble members on three grids in one
 captured CUDA graph.
 Multi-GPU: columns shard across ranks with no collective on the data path
-(weak scaling: each rank runs its own 64,800-column batch).
+(weak scaling: rank r owns columns [r*64,800, (r+1)*64,800) of a global grid,
+mgcm_rt.shard.column_shard; timings are the max over ranks).
 
 --impl reference times the reference algorithm on the host cores (the FP64
 CPU oracle -- aerosol optics and radiation, a restatement of the reference
@@ -446,7 +447,7 @@ def main():
         return
 
     import torch
-    from mgcm_rt import abi, data, synth
+    from mgcm_rt import abi, data, shard, synth
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -469,11 +470,7 @@ def main():
         torch.cuda.synchronize()
 
     def max_over_ranks(x):
-        if dist:
-            t = torch.tensor([x], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            return float(t.item())
-        return x
+        return shard.max_over_ranks(x, dist)
 
     bd = {k: (torch.from_numpy(np.ascontiguousarray(v)).to(dev) if isinstance(v, np.ndarray) else v)
           for k, v in b.items()}
