@@ -487,7 +487,7 @@ int launch_pipeline(mgcm_rt_handle *h, Slot &sl, cudaStream_t st, int total, int
     for (int c0 = 0; c0 < total; c0 += chunk) {
         const int c1 = std::min(total, c0 + chunk);
         CK(cudaMemsetAsync(counts, 0, 2 * sizeof(unsigned int), st));
-        const int g0 = std::min(c1 - c0, h->num_sms * sl.occ_stage);
+        const int g0 = std::min((c1 - c0 + 3) / 4, h->num_sms * sl.occ_stage);   // 4 columns per CTA
         rt_stage<<<g0, STAGE_THREADS, 0, st>>>(sl.d_segs, c0, c1, max_nl, blocks, stride, h->d_planck, h->K,
                                                sl.d_status);
         const long long items = (long long)(c1 - c0) * SCREEN_GROUPS;

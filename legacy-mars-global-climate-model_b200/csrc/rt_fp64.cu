@@ -86,16 +86,34 @@ rt_fp64_kernel(const SegTable *__restrict__ st, const double *__restrict__ kv,
 // per-system midpoint fluxes.  Solved systems are listed per family so the
 // solver keeps every thread busy (night columns and TLIMIT skips drop out).
 
-// K0: stage every column (bins, per-band opacity terms, Planck terms) into
-// its global block; one CTA per column.
+// K0: stage the columns (bins, per-band opacity terms, Planck terms) into
+// their global blocks, STAGE_COLS columns per CTA at a time: the level items
+// of all of them, a barrier, then their band items.
+constexpr int STAGE_COLS = 4;
+
 __global__ void __launch_bounds__(256)
 rt_stage(const SegTable *__restrict__ st, int col_begin, int col_end, int max_nl,
          unsigned char *__restrict__ blocks, size_t stride, const double *__restrict__ planck,
          const RtConst K, uint32_t *status) {
-    for (int g = col_begin + blockIdx.x; g < col_end; g += gridDim.x) {
-        const SegDev &sg = st->seg[find_seg(st, g)];
-        ColSmem s = carve_smem(blocks + (size_t)(g - col_begin) * stride, max_nl, nullptr, false);
-        stage_column(sg, g - sg.col0, K, planck, s, status);
+    const int per_lev = 2 * max_nl + 1;                             // k = 2 .. 2NL+2
+    const int per_band = (max_nl + 1) * (D_NV + D_NI) + D_NI;       // stage_band_items(max L)
+    for (int g0 = col_begin + blockIdx.x * STAGE_COLS; g0 < col_end; g0 += gridDim.x * STAGE_COLS) {
+        const int ng = min(STAGE_COLS, col_end - g0);
+        for (int it = threadIdx.x; it < ng * per_lev; it += blockDim.x) {
+            const int g = g0 + it / per_lev, k = 2 + it % per_lev;
+            const SegDev &sg = st->seg[find_seg(st, g)];
+            if (k > 2 * sg.L + 4) continue;
+            ColSmem s = carve_smem(blocks + (size_t)(g - col_begin) * stride, max_nl, nullptr, false);
+            stage_level(sg, g - sg.col0, K, s, k);
+        }
+        __syncthreads();
+        for (int it = threadIdx.x; it < ng * per_band; it += blockDim.x) {
+            const int g = g0 + it / per_band, j = it % per_band;
+            const SegDev &sg = st->seg[find_seg(st, g)];
+            if (j >= stage_band_items(sg.L)) continue;
+            ColSmem s = carve_smem(blocks + (size_t)(g - col_begin) * stride, max_nl, nullptr, false);
+            stage_band(sg, g - sg.col0, K, planck, s, j, status);
+        }
         __syncthreads();
     }
 }

@@ -7,11 +7,9 @@
 
 namespace mgcm {
 
-__device__ inline void stage_column(const SegDev &sg, int c, const RtConst &K,
-                                    const double *__restrict__ planck, ColSmem &s,
-                                    uint32_t *status) {
-    const int L = sg.L, NL = L + 1, LEV = 2 * L + 3, LEV1 = LEV + 1;
-    const int tid = threadIdx.x, nth = blockDim.x;
+// Level item k (2..LEV+1) of column c: bins, U, DPR and the TAUREF ratios.
+__device__ inline void stage_level(const SegDev &sg, int c, const RtConst &K, ColSmem &s, int k) {
+    const int L = sg.L, LEV = 2 * L + 3, LEV1 = LEV + 1;
     const double *plev = sg.plev + (size_t)c * LEV;
     const double *tlev = sg.tlev + (size_t)c * LEV;
     const double *pmid = sg.pmid + (size_t)c * LEV;
@@ -24,8 +22,7 @@ __device__ inline void stage_column(const SegDev &sg, int c, const RtConst &K,
     const double *taucld = cld ? sg.taurefcld + (size_t)c * LEV1 : nullptr;
     const double *qxcld = cld ? sg.qextrefcld + (size_t)c * LEV1 : nullptr;
 
-    // level items: k = 2..LEV (bins, U, DPR, TAUREF ratios); k = LEV+1 raw values (IR)
-    for (int k = 2 + tid; k <= LEV1; k += nth) {
+    {
         if (k <= LEV) {
             int mt, mp, nh;
             double wr, lk[4];
@@ -49,11 +46,21 @@ __device__ inline void stage_column(const SegDev &sg, int c, const RtConst &K,
             s.tref_c[k] = cld ? taucld[k - 1] : 0.0;
         }
     }
-    __syncthreads();
+}
 
-    // band items.  Visible layer l (1..NL) and level 2 (l = 0); IR likewise.
+// Band items of a column: nitem_v = (NL+1)*7 visible (layer l = 0..NL: level 2
+// for l = 0), nitem_i = (NL+1)*5 IR with the Planck terms, then 5 IR boundary
+// items.  Needs every level item of the column staged first.
+__device__ __forceinline__ int stage_band_items(int L) { return (L + 2) * (D_NV + D_NI) + D_NI; }
+
+__device__ inline void stage_band(const SegDev &sg, int c, const RtConst &K,
+                                  const double *__restrict__ planck, ColSmem &s, int it,
+                                  uint32_t *status) {
+    const int L = sg.L, NL = L + 1, LEV = 2 * L + 3, LEV1 = LEV + 1;
+    const double *tlev = sg.tlev + (size_t)c * LEV;
+    const bool cld = sg.taurefcld != nullptr;
     const int nitem_v = (NL + 1) * D_NV, nitem_i = (NL + 1) * D_NI;
-    for (int it = tid; it < nitem_v + nitem_i + D_NI; it += nth) {
+    {
         if (it < nitem_v) {
             const int l = it / D_NV, nw = it % D_NV + 1;
             const double *qx = sg.qxvdst + ((size_t)c * D_NV + nw - 1) * LEV1;
@@ -143,6 +150,17 @@ __device__ inline void stage_column(const SegDev &sg, int c, const RtConst &K,
             s.pltop_i[nw - 1] = planck[(ntt - 1) * D_NI + nw - 1];
         }
     }
+}
+
+// The whole column by one CTA (the fused kernel).
+__device__ inline void stage_column(const SegDev &sg, int c, const RtConst &K,
+                                    const double *__restrict__ planck, ColSmem &s,
+                                    uint32_t *status) {
+    const int LEV1 = 2 * sg.L + 4;
+    for (int k = 2 + (int)threadIdx.x; k <= LEV1; k += blockDim.x) stage_level(sg, c, K, s, k);
+    __syncthreads();
+    const int n = stage_band_items(sg.L);
+    for (int it = threadIdx.x; it < n; it += blockDim.x) stage_band(sg, c, K, planck, s, it, status);
 }
 
 }  // namespace mgcm
