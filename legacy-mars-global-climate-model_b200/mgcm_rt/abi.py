@@ -10,13 +10,15 @@ itself.  There is no CPU fallback: a missing library raises at import.
 from __future__ import annotations
 
 import ctypes as C
+import os
 import pathlib
 
 import numpy as np
 
 from . import INPUT_COL, INPUT_LEV, OUTPUT_COL, OUTPUT_LAY
 
-LIB_PATH = pathlib.Path(__file__).resolve().parent / "libmgcmrt.so"
+LIB_PATH = (pathlib.Path(os.environ["MGCM_RT_LIBRARY"]) if os.environ.get("MGCM_RT_LIBRARY")
+            else pathlib.Path(__file__).resolve().parent / "libmgcmrt.so")
 
 FP64, MIXED = 0, 1
 STATUS = {0: "OK", -1: "EINVAL", -2: "ENONFINITE", -3: "ETEMP", -4: "ELAYERS", -5: "ENOMEM",
