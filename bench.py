@@ -49,8 +49,9 @@ WORKLOADS = {
                name="180x360 = 64,800 columns x 24 layers, dust + water-ice cloud, half night"),
     "c0": dict(ncol=2160, L=24, cloud=False,
                name="36x60 = 2,160 columns x 24 layers, dust only, half night"),
-    "c4": dict(ncol=1036800 // 8, L=48, cloud=True,
-               name="720x1440 x 48 layers, one eighth (129,600 columns) per call"),
+    "c4": dict(ncol=1036800, L=48, cloud=True, tile=20000,
+               name="720x1440 = 1,036,800 columns x 48 layers, dust + water-ice cloud, one call "
+                    "(inputs tiled on the device from a seeded 20,000-column batch)"),
     # 64 ensemble members of uneven grids in one captured graph (see run_ensemble)
     "c2": dict(ncol=889920, L=48, cloud=True,
                name="64 members: 4 x 36x60x24 + 12 x 72x120x36 + 48 x 90x180x48 = 889,920 columns, "
@@ -73,13 +74,15 @@ def algorithmic_bytes_per_column(L: int, cloud: bool) -> int:
     return 8 * (n_in + n_out + n_state)
 
 
-def traffic_per_step(precision: str, ncol: int):
+def traffic_per_step(precision: str, ncol: int, layers: int):
     """DRAM bytes (read + write) of one call's kernels from the committed ncu
-    summary (profiles/pipeline_traffic.json, an 8,192-column capture), scaled
-    to `ncol` columns; None when absent."""
+    summary (profiles/pipeline_traffic.json, an 8,192-column L = 24 capture),
+    scaled to `ncol` columns of the same layer count; None otherwise."""
     try:
         j = json.loads((ROOT / "profiles" / "pipeline_traffic.json").read_text())
         e = j[precision]
+        if int(e["layers"]) != layers:
+            return None
         return float(e["dram_bytes"]) * ncol / float(e["columns"])
     except Exception:
         return None
@@ -461,7 +464,8 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     d, kind = data.ensure_data()
     L, ncol = wl["L"], wl["ncol"]
-    b = synth.make_batch(ncol, L=L, seed=1000 + rank, cloud=wl["cloud"])
+    tile = wl.get("tile")
+    b = synth.make_batch(tile or ncol, L=L, seed=1000 + rank, cloud=wl["cloud"])
     stream = torch.cuda.Stream()
 
     def barrier():
@@ -474,6 +478,12 @@ def main():
 
     bd = {k: (torch.from_numpy(np.ascontiguousarray(v)).to(dev) if isinstance(v, np.ndarray) else v)
           for k, v in b.items()}
+    if tile:   # a grid too large for the host: repeat the seeded batch on the device
+        rep = (ncol + tile - 1) // tile
+        bd = {k: (v.repeat((rep,) + (1,) * (v.dim() - 1))[:ncol].contiguous()
+                  if torch.is_tensor(v) and k not in ("sigma", "sol") else v) for k, v in bd.items()}
+        bd["ncol"] = ncol
+        args.no_e2e = args.no_serving = True   # host-buffer legs need the whole grid on the host
     precs = ["fp64", "mixed"] if args.precision == "both" else [args.precision]
     res, outs, handles = {}, {}, {}
     clk_summary = None
@@ -575,11 +585,11 @@ def main():
                     else "synthetic (seeded; synthetic k tables)",
             "config": {"workload": wl["name"], "columns_per_gpu": ncol, "layers": L,
                        "precision": hp, "k_tables": kind,
-                       "l2": "inputs 2.5 GB per step > 126 MB L2 (no flush needed)",
+                       "l2": f"inputs {bpc * ncol / 1e9:.1f} GB per step > 126 MB L2 (no flush needed)",
                        "parallelism": f"column shards x{world}, no collective"},
             "gpu_launches": args.steps * int(st["kernels"]),
             "roofline": {"bound": "hbm", "achieved": ach, "peak": pk, "unit": "GB/s",
-                         "frac": ach / pk, "traffic": traffic_per_step(hp, ncol),
+                         "frac": ach / pk, "traffic": traffic_per_step(hp, ncol, L),
                          "kernel": "radiation pipeline (stage, screen, 2 solves, reduce) per call",
                          "bytes_per_column": bpc, "kernel_ms": kms, "peak_kind": pk_kind},
             "systems_per_step": st["systems"],
