@@ -175,6 +175,8 @@ struct Tune {
 
 struct Slot {
     cudaStream_t stream = nullptr;
+    cudaStream_t aux = nullptr;   // the visible solve runs here, beside the IR solve
+    cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, done = nullptr;
     SegTable *h_segs = nullptr, *d_segs = nullptr;
     uint32_t *d_status = nullptr, *h_status = nullptr;
@@ -374,6 +376,9 @@ int arena_ensure(mgcm_rt_handle *h, Arena &a, size_t bytes, cudaStream_t s) {
 
 int slot_init(Slot &s) {
     CK(cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&s.aux, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&s.fork_ev, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&s.join_ev, cudaEventDisableTiming));
     CK(cudaEventCreate(&s.ev0));
     CK(cudaEventCreate(&s.ev1));
     CK(cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming));
@@ -404,6 +409,10 @@ void slot_free(mgcm_rt_handle *h, Slot &s) {
     if (s.ev0) cudaEventDestroy(s.ev0);
     if (s.ev1) cudaEventDestroy(s.ev1);
     if (s.done) cudaEventDestroy(s.done);
+    if (s.aux) cudaStreamSynchronize(s.aux);
+    if (s.fork_ev) cudaEventDestroy(s.fork_ev);
+    if (s.join_ev) cudaEventDestroy(s.join_ev);
+    if (s.aux) cudaStreamDestroy(s.aux);
     if (s.stream) cudaStreamDestroy(s.stream);
 }
 
@@ -502,17 +511,22 @@ int launch_pipeline(mgcm_rt_handle *h, Slot &sl, cudaStream_t st, int total, int
                                                                  h->d_kv, h->d_ki, h->K, list_v, list_i,
                                                                  counts, sl.d_nsys, nullptr);
         const int g2 = h->num_sms * (sl.tune.solve_ctas > 0 ? sl.tune.solve_ctas : sl.occ_solve);
-        // MIXED: FP32 visible opacities; the IR family is FP64 in both modes
+        // MIXED: FP32 visible opacities; the IR family is FP64 in both modes.
+        // The visible solve runs on the slot's second stream beside the IR
+        // solve, so each kernel's last wave overlaps the other's.
+        CK(cudaEventRecord(sl.fork_ev, st));
+        CK(cudaStreamWaitEvent(sl.aux, sl.fork_ev, 0));
+        cudaStream_t vst = sl.aux;
         const int qr = h->quad ? quad_r_for(max_nl) : 0;
         if (qr) {
             const int gq = h->num_sms * (sl.tune.solve_ctas > 0 ? sl.tune.solve_ctas : sl.occ_quad);
 #define MGCM_QUAD(R)                                                                                        \
     do {                                                                                                    \
         if (mixed)                                                                                          \
-            rt_quad_mixed_vis<R><<<gq, 128, 0, st>>>(sl.d_segs, c0, max_nl, blocks, stride, h->d_kvf,        \
+            rt_quad_mixed_vis<R><<<gq, 128, 0, vst>>>(sl.d_segs, c0, max_nl, blocks, stride, h->d_kvf,       \
                                                      h->d_kv, h->K, list_v, counts, fl_v, sc_v);             \
         else                                                                                                \
-            rt_quad_solve<true, R><<<gq, 128, 0, st>>>(sl.d_segs, c0, max_nl, blocks, stride, h->d_kv, h->K, \
+            rt_quad_solve<true, R><<<gq, 128, 0, vst>>>(sl.d_segs, c0, max_nl, blocks, stride, h->d_kv, h->K,\
                                                        list_v, counts, fl_v, sc_v);                          \
         rt_quad_solve<false, R><<<gq, 128, 0, st>>>(sl.d_segs, c0, max_nl, blocks, stride, h->d_ki, h->K,    \
                                                     list_i, counts, fl_i, sc_i);                             \
@@ -523,14 +537,17 @@ int launch_pipeline(mgcm_rt_handle *h, Slot &sl, cudaStream_t st, int total, int
 #undef MGCM_QUAD
         } else {
             if (mixed)
-                rt_mixed_solve_vis<<<g2, 128, 0, st>>>(sl.d_segs, c0, max_nl, blocks, stride, h->d_kvf, h->d_kv,
-                                                       h->K, list_v, counts, fl_v, sc_v);
+                rt_mixed_solve_vis<<<g2, 128, 0, vst>>>(sl.d_segs, c0, max_nl, blocks, stride, h->d_kvf, h->d_kv,
+                                                        h->K, list_v, counts, fl_v, sc_v);
             else
-                rt_fp64_solve<true><<<g2, 128, 0, st>>>(sl.d_segs, c0, max_nl, blocks, stride, h->d_kv, h->K,
-                                                        list_v, counts, fl_v, sc_v);
+                rt_fp64_solve<true><<<g2, 128, 0, vst>>>(sl.d_segs, c0, max_nl, blocks, stride, h->d_kv, h->K,
+                                                         list_v, counts, fl_v, sc_v);
             rt_fp64_solve<false><<<g2, 128, 0, st>>>(sl.d_segs, c0, max_nl, blocks, stride, h->d_ki, h->K,
                                                      list_i, counts, fl_i, sc_i);
         }
+        CK(cudaGetLastError());
+        CK(cudaEventRecord(sl.join_ev, sl.aux));
+        CK(cudaStreamWaitEvent(st, sl.join_ev, 0));
         const int g3 = std::min((c1 - c0 + REDUCE_WARPS - 1) / REDUCE_WARPS, h->num_sms * sl.occ_reduce);
         rt_fp64_reduce<<<g3, REDUCE_THREADS, rsm, st>>>(sl.d_segs, c0, c1, max_nl, blocks, stride, h->K,
                                                         fl_v, sc_v, fl_i, sc_i, sl.d_status, rb);
