@@ -68,6 +68,7 @@ __global__ void rt_mixed_solve_vis(const SegTable *__restrict__ st, int col_begi
                                    const RtConst K, const int *__restrict__ list,
                                    const unsigned int *count, double *__restrict__ fl,
                                    double *__restrict__ sc);
+template <bool ONE_LEVEL>
 __global__ void rt_fp64_reduce(const SegTable *__restrict__ st, int col_begin, int col_end,
                                int max_nl, unsigned char *__restrict__ blocks, size_t stride,
                                const RtConst K, const double *__restrict__ fl_v,
@@ -425,7 +426,8 @@ int configure_kernels(int device) {
     std::lock_guard<std::mutex> lk(mu);
     if (device < 0 || device >= 256) return MGCM_RT_EINVAL;
     if (done[device]) return MGCM_RT_OK;
-    CK(cudaFuncSetAttribute(rt_fp64_reduce, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_CAP));
+    CK(cudaFuncSetAttribute(rt_fp64_reduce<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_CAP));
+    CK(cudaFuncSetAttribute(rt_fp64_reduce<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_CAP));
     CK(cudaFuncSetAttribute(rt_fp64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_CAP));
     // the solvers use no shared memory: the whole unified L1 goes to the
     // per-system arrays
@@ -488,7 +490,8 @@ int launch_pipeline(mgcm_rt_handle *h, Slot &sl, cudaStream_t st, int total, int
         else if (qr == 10) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&qo, rt_quad_solve<false, 10>, 128, 0);
         else if (qr == 13) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&qo, rt_quad_solve<false, 13>, 128, 0);
         sl.occ_quad = std::max(qo, 1);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, rt_fp64_reduce, REDUCE_THREADS, rsm);
+        if (max_nl <= 32) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, rt_fp64_reduce<true>, REDUCE_THREADS, rsm);
+        else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, rt_fp64_reduce<false>, REDUCE_THREADS, rsm);
         sl.occ_screen = std::max(a, 1);
         sl.occ_solve = std::max(b, 1);
         sl.occ_reduce = std::max(c, 1);
@@ -549,8 +552,12 @@ int launch_pipeline(mgcm_rt_handle *h, Slot &sl, cudaStream_t st, int total, int
         CK(cudaEventRecord(sl.join_ev, sl.aux));
         CK(cudaStreamWaitEvent(st, sl.join_ev, 0));
         const int g3 = std::min((c1 - c0 + REDUCE_WARPS - 1) / REDUCE_WARPS, h->num_sms * sl.occ_reduce);
-        rt_fp64_reduce<<<g3, REDUCE_THREADS, rsm, st>>>(sl.d_segs, c0, c1, max_nl, blocks, stride, h->K,
-                                                        fl_v, sc_v, fl_i, sc_i, sl.d_status, rb);
+        if (max_nl <= 32)
+            rt_fp64_reduce<true><<<g3, REDUCE_THREADS, rsm, st>>>(sl.d_segs, c0, c1, max_nl, blocks, stride, h->K,
+                                                                  fl_v, sc_v, fl_i, sc_i, sl.d_status, rb);
+        else
+            rt_fp64_reduce<false><<<g3, REDUCE_THREADS, rsm, st>>>(sl.d_segs, c0, c1, max_nl, blocks, stride, h->K,
+                                                                   fl_v, sc_v, fl_i, sc_i, sl.d_status, rb);
         nk += 5;
         CK(cudaGetLastError());
     }

@@ -341,6 +341,7 @@ __device__ inline void warp_multipliers(const unsigned char *skip, bool day, con
     p3[pos] = 1.0;
 }
 
+template <bool ONE_LEVEL>   // max NL <= 32: one level per lane
 __global__ void __launch_bounds__(32 * RED_WARPS)
 rt_fp64_reduce(const SegTable *__restrict__ st, int col_begin, int col_end, int max_nl,
                unsigned char *__restrict__ blocks, size_t stride, const RtConst K,
@@ -481,22 +482,40 @@ rt_fp64_reduce(const SegTable *__restrict__ st, int col_begin, int col_end, int 
                          *f3 = (vis ? m3 : m3 + NSYS_V) + r0;
             for (int k = 0; k < cnt; ++k) {
                 const double a = f1[k], b = f2[k], e = f3[k];
+                // ((v*a)*b)*e in the reference order; a factor that is exactly
+                // 1.0 leaves the product unchanged and is skipped (warp-uniform)
+                const bool b1 = b == 1.0, e1 = e == 1.0;
+                auto wt = [&](double v) {
+                    double x = v * a;
+                    if (!b1) x = x * b;
+                    if (!e1) x = x * e;
+                    return x;
+                };
                 const double *pr = buf + (size_t)k * row;
+                if (ONE_LEVEL) {
+                    if (lane < NL) {
+                        const double up = pr[lane], dn = pr[max_nl + lane];
+                        acc[0][0] = acc[0][0] + wt(up - dn);
+                        acc[1][0] = acc[1][0] + wt(up);
+                        acc[2][0] = acc[2][0] + wt(dn);
+                    }
+                } else {
 #pragma unroll
-                for (int r = 0; r < RED_LPL; ++r) {
-                    const int l = lane + 1 + 32 * r;
-                    if (l > NL) break;
-                    const double up = pr[l - 1], dn = pr[max_nl + l - 1];
-                    acc[0][r] = acc[0][r] + (up - dn) * a * b * e;
-                    acc[1][r] = acc[1][r] + up * a * b * e;
-                    acc[2][r] = acc[2][r] + dn * a * b * e;
+                    for (int r = 0; r < RED_LPL; ++r) {
+                        const int l = lane + 1 + 32 * r;
+                        if (l > NL) break;
+                        const double up = pr[l - 1], dn = pr[max_nl + l - 1];
+                        acc[0][r] = acc[0][r] + wt(up - dn);
+                        acc[1][r] = acc[1][r] + wt(up);
+                        acc[2][r] = acc[2][r] + wt(dn);
+                    }
                 }
                 const double *sk = scb + (size_t)k * 4;
                 if (vis) {
-                    top = top + (sk[0] - sk[1]) * a * b * e;
-                    dif = dif + sk[2] * a * b * e;
+                    top = top + wt(sk[0] - sk[1]);
+                    dif = dif + wt(sk[2]);
                 } else {
-                    top = top + sk[0] * a * b * e;
+                    top = top + wt(sk[0]);
                 }
             }
             ++gc;
@@ -529,6 +548,14 @@ rt_fp64_reduce(const SegTable *__restrict__ st, int col_begin, int col_end, int 
         __syncwarp();
     }
 }
+
+#define REDUCE_ARGS                                                                                    \
+    const SegTable *__restrict__, int, int, int, unsigned char *__restrict__, size_t, const RtConst,  \
+        const double *__restrict__, const double *__restrict__, const double *__restrict__,          \
+        const double *__restrict__, uint32_t *, int
+template __global__ void rt_fp64_reduce<true>(REDUCE_ARGS);
+template __global__ void rt_fp64_reduce<false>(REDUCE_ARGS);
+#undef REDUCE_ARGS
 
 // Shared memory of rt_fp64_reduce with `rb` rows per chunk.
 size_t reduce_smem_bytes(int max_nl, int rb) { return (size_t)RED_WARPS * red_warp_bytes(max_nl, rb); }
