@@ -90,7 +90,7 @@ using namespace mgcm;
 namespace {
 
 constexpr int BLOCK = 224;
-constexpr int SYNC_JOB_COLS = 16384;    // columns per job of a synchronous host-buffer call
+constexpr int SYNC_JOB_COLS = 8192;     // columns per job of a synchronous host-buffer call (measured best of 2k-32k)
 constexpr int SERVE_JOB_COLS = 32768;   // columns per job of a served request
 constexpr int SERVE_SLOTS = 4;          // serving slots at most
 
