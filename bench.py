@@ -561,10 +561,38 @@ def main():
         e1.record(stream)
         barrier()
         tms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+        # the same columns through mgcm_rt_run_state: the GCM state (layer
+        # temperatures, P, TSTRAT, GT, vapour, TAUTOT) and the ice tracers;
+        # the column prep (FILLPT, QH2O, DUSTPROFILE + FILLTAUCUM) runs on the
+        # device too
+        sb = synth.make_state_batch(ncol, L=L, seed=1000 + rank, active_dust=False, cloudon=wl["cloud"])
+        hs = {}
+        for k, v in sb.items():
+            if isinstance(v, np.ndarray):
+                tpin = torch.empty(v.shape, dtype=torch.float64, pin_memory=True)
+                tpin.numpy()[...] = v
+                keep.append(tpin)
+                hs[k] = tpin.numpy()
+            else:
+                hs[k] = v
+        h2d_s = sum(v.nbytes for v in hs.values() if isinstance(v, np.ndarray))
+        for _ in range(args.warmup):
+            rt.run_state(hs, ho, inplace=True)
+        barrier()
+        e0.record(stream)
+        for _ in range(args.steps):
+            rt.run_state(hs, ho, inplace=True)
+        e1.record(stream)
+        barrier()
+        sms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+        e2e_state = {"value": ncol * world / (sms / 1e3), "unit": UNIT, "h2d_bytes_per_step": int(h2d_s),
+                     "d2h_bytes_per_step": int(d2h), "ms_per_step": sms,
+                     "path": f"mgcm_rt_run_state ({hp}): GCM state inputs, column prep and aerosol "
+                             "optics on the device"}
         e2e = {"value": ncol * world / (tms / 1e3), "unit": UNIT, "h2d_bytes_per_step": int(h2d_t),
                "d2h_bytes_per_step": int(d2h), "ms_per_step": tms,
                "path": f"mgcm_rt_run_tracers ({hp}): tracer inputs, aerosol optics on the device",
-               "arrays_path": e2e_arrays}
+               "arrays_path": e2e_arrays, "state_path": e2e_state}
 
     acc = None
     if "fp64" in outs and "mixed" in outs:

@@ -187,6 +187,43 @@ typedef struct {
 } mgcm_rt_batch_tracers;
 int mgcm_rt_run_tracers(mgcm_rt_handle *h, const mgcm_rt_batch_tracers *in, mgcm_rt_batch_out *out);
 
+/* ---- GCM state inputs: column prep on the device ------------------------
+ * COMP3's assembly of the radiation inputs runs on the device as well: the
+ * level pressures PL (code/potemp1.f:95-106) and FILLPT's PLEV, TLEV, PMID,
+ * TMID (code/fillpt.f90:30-72), QH2O (code/comp3.f:576-589) and, for
+ * prescribed dust, TAUREF from the Conrath profile of DUSTPROFILE sampled by
+ * FILLTAUCUM (code/dustprofile.f:88-172, code/filltaucum.f:39-55).  Then the
+ * aerosol optics and the radiation run as in mgcm_rt_run_tracers.  The host
+ * passes the model state itself: about 1.6 KB per column at L = 24 with
+ * dust and ice tracers.  COLDAIR stays on the host (it changes the model
+ * state); t, tstrat and gt are its results.  The prepared level arrays can
+ * be returned through the optional pointers.  No reference counterpart as
+ * one call; the outputs equal mgcm_rt_run_tracers on the same prepared
+ * arrays. */
+typedef struct {
+    int ncol, nlayers, device_ptrs;
+    int active_dust;     /* 1: OPT_DST from the dust tracers; 0: prescribed (Conrath) dust */
+    int cloudon;         /* 1: OPT_CLD from the ice tracers; 0: no cloud */
+    int active_water;    /* 1: QH2O = mwratio * vapour; 0: QH2O = 1.0E-7 (REAL*4) */
+    double ptrop;        /* PTROP (mbar) */
+    double psf;          /* PSF (mbar): sets the PRDST grid of the dust profile (active_dust = 0) */
+    double rptau;        /* RPTAU (mbar): pressure tautot refers to (active_dust = 0) */
+    double mwratio;      /* MWRATIO = MWCO2/MWH2O, code/input.f:180 (active_water = 1) */
+    const double *sigma, *sol;                    /* [2L+3] SIGMA, [7] SOLARF/RSDIST */
+    const double *pcol;                           /* [ncol] P(J,I) (mbar) */
+    const double *t;                              /* [ncol][L] TL(2l+2) = T(J,I,l) after COLDAIR */
+    const double *tstrat, *gt;                    /* [ncol] TSTRAT(J,I), GT(J,I) after COLDAIR */
+    const double *vapour;                         /* [ncol][L] QTRACE(J,I,L,iMa_vap) (active_water = 1) */
+    const double *tautot, *conr;                  /* [ncol] TAUTOTJI(J,I), Conrath nu (active_dust = 0) */
+    const double *dust_mass, *dust_number;        /* [ncol][L] (active_dust = 1) */
+    const double *ice_mass, *ice_core_mass, *ice_number; /* [ncol][L] (cloudon = 1) */
+    const double *acosz, *als, *albi;             /* [ncol] */
+    double *detau, *cumtauv;                      /* [ncol][17][7] in/out */
+    double *plev, *tlev, *pmid, *tmid, *qh2o;     /* [ncol][2L+3] optional out (NULL: not returned) */
+    double *tauref;                               /* [ncol][2L+4] optional out (active_dust = 0) */
+} mgcm_rt_batch_state;
+int mgcm_rt_run_state(mgcm_rt_handle *h, const mgcm_rt_batch_state *in, mgcm_rt_batch_out *out);
+
 /* ---- captured uneven batches ------------------------------------------
  * A fixed set of device-resident batches (e.g. the members of an ensemble,
  * grids of different layer counts) captured once as a CUDA graph and

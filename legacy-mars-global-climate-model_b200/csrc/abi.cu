@@ -27,6 +27,7 @@
 
 #include "../../include/mgcm_rt.h"
 #include "rt_aerosol.cuh"
+#include "rt_prep.cuh"
 #include "rt_column.cuh"
 #include "tables.h"
 
@@ -792,11 +793,67 @@ int check_tracers(const mgcm_rt_handle *h, const mgcm_rt_batch_tracers *in, cons
     return MGCM_RT_OK;
 }
 
+// A state batch as the tracer batch it becomes once rt_prep has filled the
+// level arrays (those pointers stay NULL here).
+mgcm_rt_batch_tracers tracers_of_state(const mgcm_rt_batch_state &s) {
+    mgcm_rt_batch_tracers t{};
+    t.ncol = s.ncol;
+    t.nlayers = s.nlayers;
+    t.device_ptrs = s.device_ptrs;
+    t.active_dust = s.active_dust;
+    t.cloudon = s.cloudon;
+    t.ptrop = s.ptrop;
+    t.sigma = s.sigma;
+    t.sol = s.sol;
+    t.dust_mass = s.dust_mass;
+    t.dust_number = s.dust_number;
+    t.ice_mass = s.ice_mass;
+    t.ice_core_mass = s.ice_core_mass;
+    t.ice_number = s.ice_number;
+    t.acosz = s.acosz;
+    t.als = s.als;
+    t.albi = s.albi;
+    t.pcol = s.pcol;
+    t.detau = s.detau;
+    t.cumtauv = s.cumtauv;
+    return t;
+}
+
+int check_state(const mgcm_rt_handle *h, const mgcm_rt_batch_state *in, const mgcm_rt_batch_out *out) {
+    if (!h || !in || !out) return MGCM_RT_EINVAL;
+    if (in->ncol < 0) return MGCM_RT_EINVAL;
+    if (in->nlayers < 1 || in->nlayers > MGCM_RT_MAX_LAYERS || in->nlayers > h->cfg.max_layers)
+        return MGCM_RT_ELAYERS;
+    if (in->ncol == 0) return MGCM_RT_OK;
+    const void *req[] = {in->sigma, in->sol, in->pcol, in->t, in->tstrat, in->gt, in->acosz, in->als,
+                         in->albi, in->detau, in->cumtauv, out->fmnetv, out->fluxupv, out->fluxdnv,
+                         out->fmneti, out->fluxupi, out->fluxdni, out->suntot, out->irtotal, out->qrad,
+                         out->nfluxtopv, out->nfluxtopi, out->diffvt, out->dnvflux, out->dndiffv,
+                         out->dnirflux, out->fluxsurf};
+    for (const void *p : req)
+        if (!p) return MGCM_RT_EINVAL;
+    if (in->active_water && !in->vapour) return MGCM_RT_EINVAL;
+    if (in->active_dust ? (!in->dust_mass || !in->dust_number) : (!in->tautot || !in->conr))
+        return MGCM_RT_EINVAL;
+    if (in->cloudon && (!in->ice_mass || !in->ice_core_mass || !in->ice_number)) return MGCM_RT_EINVAL;
+    if (!std::isfinite(in->ptrop) || !(in->ptrop > 0.0)) return MGCM_RT_ENONFINITE;
+    if (!in->active_dust && (!std::isfinite(in->psf) || !(in->psf > 0.0) || !std::isfinite(in->rptau) ||
+                             !(in->rptau > 0.0)))
+        return MGCM_RT_ENONFINITE;
+    if (in->active_water && !std::isfinite(in->mwratio)) return MGCM_RT_ENONFINITE;
+    if (!h->d_mie) return MGCM_RT_EIO;
+    return MGCM_RT_OK;
+}
+
 // One job of a tracer batch on a slot: compact inputs staged (host) or
 // offset (device), the aerosol arrays filled by rt_aerosol, the pipeline,
-// outputs copied back (host); records sl.done.
+// outputs copied back (host); records sl.done.  With a state batch (stt) the
+// level arrays and the prescribed TAUREF are not inputs: rt_prep builds them
+// from the column state first (into the caller's optional outputs, or the
+// slot's aerosol arena).
 int issue_tracer_job(mgcm_rt_handle *h, Slot &sl, cudaStream_t st, const mgcm_rt_batch_tracers &in,
-                     const mgcm_rt_batch_out &out, int c0, int c1) {
+                     const mgcm_rt_batch_out &out, int c0, int c1,
+                     const mgcm_rt_batch_state *stt = nullptr) {
     const size_t n = (size_t)(c1 - c0);
     const int L = in.nlayers, lev = 2 * L + 3, lev1 = lev + 1, nl = L + 1;
     SegDev sd{};
@@ -814,12 +871,44 @@ int issue_tracer_job(mgcm_rt_handle *h, Slot &sl, cudaStream_t st, const mgcm_rt
         if (p) arrs.push_back({p, nullptr, per, 0, const_cast<double **>(f)});
     };
     auto add_out = [&](double *p, size_t per, double **f) { arrs.push_back({nullptr, p, per, 1, f}); };
-    add_in(in.plev, lev, &sd.plev);
-    add_in(in.tlev, lev, &sd.tlev);
-    add_in(in.pmid, lev, &sd.pmid);
-    add_in(in.tmid, lev, &sd.tmid);
-    add_in(in.qh2o, lev, &sd.qh2o);
-    if (!in.active_dust) add_in(in.tauref, lev1, &as.tauref_in);
+    PrepSeg ps{};
+    // prepared arrays the caller asked for (the others go to the arena below)
+    double *prep_want[6] = {};
+    double **prep_field[6] = {const_cast<double **>(&sd.plev), const_cast<double **>(&sd.tlev),
+                              const_cast<double **>(&sd.pmid), const_cast<double **>(&sd.tmid),
+                              const_cast<double **>(&sd.qh2o), const_cast<double **>(&as.tauref_in)};
+    if (!stt) {
+        add_in(in.plev, lev, &sd.plev);
+        add_in(in.tlev, lev, &sd.tlev);
+        add_in(in.pmid, lev, &sd.pmid);
+        add_in(in.tmid, lev, &sd.tmid);
+        add_in(in.qh2o, lev, &sd.qh2o);
+        if (!in.active_dust) add_in(in.tauref, lev1, &as.tauref_in);
+    } else {
+        ps.ncol = (int)n;
+        ps.L = L;
+        ps.active_water = stt->active_water ? 1 : 0;
+        ps.prescribed_dust = stt->active_dust ? 0 : 1;
+        ps.ptrop = stt->ptrop;
+        ps.psf = stt->psf;
+        ps.rptau = stt->rptau;
+        ps.mwratio = stt->mwratio;
+        add_in(stt->t, L, &ps.t);
+        add_in(stt->tstrat, 1, &ps.tstrat);
+        add_in(stt->gt, 1, &ps.gt);
+        if (ps.active_water) add_in(stt->vapour, L, &ps.vapour);
+        if (ps.prescribed_dust) {
+            add_in(stt->tautot, 1, &ps.tautot);
+            add_in(stt->conr, 1, &ps.conr);
+        }
+        double *want[6] = {stt->plev, stt->tlev, stt->pmid, stt->tmid, stt->qh2o,
+                           ps.prescribed_dust ? stt->tauref : nullptr};
+        for (int i = 0; i < 6; ++i)
+            if (want[i]) {
+                prep_want[i] = want[i];
+                add_out(want[i], i == 5 ? lev1 : lev, prep_field[i]);
+            }
+    }
     if (in.active_dust) {
         add_in(in.dust_mass, L, &as.dust_mass);
         add_in(in.dust_number, L, &as.dust_number);
@@ -877,13 +966,29 @@ int issue_tracer_job(mgcm_rt_handle *h, Slot &sl, cudaStream_t st, const mgcm_rt
         sd.sigma = ds;
         sd.sol = ds + lev;
     }
-    // the per-level aerosol arrays of the ABI, on the device
+    // the per-level aerosol arrays of the ABI, on the device (+ the prepared
+    // level arrays of a state batch that the caller does not take)
     const size_t per = (size_t)lev1 * (2 + 3 * (AERO_NV + AERO_NI));
-    const size_t abytes = n * per * 8 * (in.cloudon ? 2 : 1);
+    const size_t prep_per = stt ? (size_t)5 * lev + lev1 : 0;
+    const size_t abytes = n * (per * (in.cloudon ? 2 : 1) + prep_per) * 8;
     int rc = arena_ensure(h, sl.aero, abytes, st);
     if (rc) return rc;
     double *ap = static_cast<double *>(sl.aero.ptr);
     auto take = [&](size_t per_col) { double *r = ap; ap += per_col * n; return r; };
+    if (stt) {
+        for (int i = 0; i < 6; ++i) {
+            double *d = take(i == 5 ? lev1 : lev);
+            if (!prep_want[i]) *prep_field[i] = d;
+        }
+        ps.sigma = sd.sigma;
+        ps.pcol = sd.pcol;
+        ps.plev = const_cast<double *>(sd.plev);
+        ps.tlev = const_cast<double *>(sd.tlev);
+        ps.pmid = const_cast<double *>(sd.pmid);
+        ps.tmid = const_cast<double *>(sd.tmid);
+        ps.qh2o = const_cast<double *>(sd.qh2o);
+        ps.tauref = const_cast<double *>(as.tauref_in);
+    }
     as.tauref = take(lev1);
     as.qextrefdst = take(lev1);
     as.qxvdst = take((size_t)AERO_NV * lev1);
@@ -925,13 +1030,19 @@ int issue_tracer_job(mgcm_rt_handle *h, Slot &sl, cudaStream_t st, const mgcm_rt
     tab.seg[0] = sd;
     CK(cudaMemcpyAsync(sl.d_segs, sl.h_segs, offsetof(SegTable, seg) + sizeof(SegDev),
                        cudaMemcpyHostToDevice, st));
+    if (stt) {
+        const int pg = (int)std::min<long long>(((long long)n + PREP_THREADS / 32 - 1) / (PREP_THREADS / 32),
+                                                (long long)h->num_sms * 16);
+        rt_prep<<<pg, PREP_THREADS, 0, st>>>(ps);
+        CK(cudaGetLastError());
+    }
     const long long items = (long long)n * (L + 1);
     const int ag = (int)std::min<long long>((items + 127) / 128, (long long)h->num_sms * 16);
     rt_aerosol<<<ag, 128, 0, st>>>(as, h->aero, h->d_mie);
     CK(cudaGetLastError());
     rc = launch_all(h, sl, st, (int)n, nl, 1 << 30);
     if (rc) return rc;
-    ++sl.kernels;
+    sl.kernels += stt ? 2 : 1;   // rt_aerosol (+ rt_prep)
     if (!in.device_ptrs)
         for (auto &a : arrs)
             if (a.dir != 0)
@@ -943,8 +1054,10 @@ int issue_tracer_job(mgcm_rt_handle *h, Slot &sl, cudaStream_t st, const mgcm_rt
     return MGCM_RT_OK;
 }
 
-// Synchronous tracer batch: jobs alternate between the two synchronous slots.
-int run_tracers(mgcm_rt_handle *h, const mgcm_rt_batch_tracers &in, mgcm_rt_batch_out &out) {
+// Synchronous tracer (or state) batch: jobs alternate between the two
+// synchronous slots.
+int run_tracers(mgcm_rt_handle *h, const mgcm_rt_batch_tracers &in, mgcm_rt_batch_out &out,
+                const mgcm_rt_batch_state *stt = nullptr) {
     cudaStream_t ust = sync_stream(h);
     CK(cudaEventRecord(h->fork, ust));
     for (auto &s : h->slots) CK(cudaStreamWaitEvent(s->stream, h->fork, 0));
@@ -961,7 +1074,7 @@ int run_tracers(mgcm_rt_handle *h, const mgcm_rt_batch_tracers &in, mgcm_rt_batc
             acc |= *sl.h_status;
             systems += (long long)*sl.h_nsys;
         }
-        const int rc = issue_tracer_job(h, sl, sl.stream, in, out, c0, c1);
+        const int rc = issue_tracer_job(h, sl, sl.stream, in, out, c0, c1, stt);
         if (rc) return rc;
         used[k & 1] = true;
         nk += sl.kernels;
@@ -1317,6 +1430,17 @@ int mgcm_rt_dsolflux(mgcm_rt_handle *h, int ncol, int device_ptrs, const double 
     if (!device_ptrs) CK(cudaMemcpyAsync(dnvflux, dout, (size_t)ncol * 8, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     return MGCM_RT_OK;
+}
+
+int mgcm_rt_run_state(mgcm_rt_handle *h, const mgcm_rt_batch_state *in, mgcm_rt_batch_out *out) {
+    const int rc = check_state(h, in, out);
+    if (rc || in->ncol == 0) return rc;
+    std::lock_guard<std::mutex> lk(h->mu);
+    if (cudaSetDevice(h->device) != cudaSuccess) return MGCM_RT_ECUDA;
+    const int prc = finish_pending(h);
+    if (prc) return prc;
+    const mgcm_rt_batch_tracers t = tracers_of_state(*in);
+    return run_tracers(h, t, *out, in);
 }
 
 int mgcm_rt_run_tracers(mgcm_rt_handle *h, const mgcm_rt_batch_tracers *in, mgcm_rt_batch_out *out) {

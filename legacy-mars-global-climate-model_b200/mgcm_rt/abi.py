@@ -73,6 +73,19 @@ class BatchTracers(C.Structure):
                 ("cloudon", C.c_int), ("ptrop", C.c_double)] + [(n, C.c_void_p) for n in _TR_PTRS]
 
 
+_ST_PTRS = ("sigma", "sol", "pcol", "t", "tstrat", "gt", "vapour", "tautot", "conr", "dust_mass",
+            "dust_number", "ice_mass", "ice_core_mass", "ice_number", "acosz", "als", "albi", "detau",
+            "cumtauv", "plev", "tlev", "pmid", "tmid", "qh2o", "tauref")
+# prepared level arrays a state call can return (the last six of _ST_PTRS)
+PREP_FIELDS = ("plev", "tlev", "pmid", "tmid", "qh2o", "tauref")
+
+
+class BatchState(C.Structure):
+    _fields_ = [("ncol", C.c_int), ("nlayers", C.c_int), ("device_ptrs", C.c_int), ("active_dust", C.c_int),
+                ("cloudon", C.c_int), ("active_water", C.c_int), ("ptrop", C.c_double), ("psf", C.c_double),
+                ("rptau", C.c_double), ("mwratio", C.c_double)] + [(n, C.c_void_p) for n in _ST_PTRS]
+
+
 class Tune(C.Structure):
     _fields_ = [("chunk_cols", C.c_int), ("solve_ctas_per_sm", C.c_int), ("reduce_rows", C.c_int),
                 ("candidates", C.c_int), ("tuning_cols", C.c_int), ("default_ms", C.c_double),
@@ -108,6 +121,7 @@ def lib():
         L.mgcm_rt_strerror.argtypes = [C.c_int]
         L.mgcm_rt_version.restype = C.c_char_p
         L.mgcm_rt_run_tracers.argtypes = [C.c_void_p, C.POINTER(BatchTracers), C.POINTER(BatchOut)]
+        L.mgcm_rt_run_state.argtypes = [C.c_void_p, C.POINTER(BatchState), C.POINTER(BatchOut)]
         L.mgcm_rt_graph_create.argtypes = [C.c_void_p, C.c_int, C.POINTER(BatchIn), C.POINTER(BatchOut),
                                            C.c_int, C.POINTER(C.c_void_p)]
         L.mgcm_rt_graph_launch.argtypes = [C.c_void_p, C.c_void_p]
@@ -302,6 +316,58 @@ class Radiation:
         if rc != 0:
             raise RTError(rc, "mgcm_rt_run_tracers")
         out["detau"], out["cumtauv"] = t["detau"], t["cumtauv"]
+        return out
+
+    def run_state(self, st: dict, out: dict | None = None, inplace: bool = False,
+                  return_levels: bool = False) -> dict:
+        """Radiation from the GCM state of each column (synth.make_state_batch
+        layout): the device builds PLEV/TLEV/PMID/TMID/QH2O (and TAUREF for
+        prescribed dust), then the aerosol optics, then the radiation.  With
+        ``return_levels`` the prepared arrays come back in ``out`` under
+        PREP_FIELDS.  Host or CUDA inputs as in run()."""
+        dev = _is_torch(st["t"]) and st["t"].is_cuda
+        if not dev and not inplace:
+            st = dict(st)
+            st["detau"] = np.array(st["detau"], dtype=np.float64, copy=True)
+            st["cumtauv"] = np.array(st["cumtauv"], dtype=np.float64, copy=True)
+        ncol, L = int(st["ncol"]), int(st["L"])
+        if out is None:
+            out = alloc_outputs(ncol, L, device=st["t"].device if dev else None)
+        prescribed = not st.get("active_dust", 0)
+        if return_levels:
+            lev = 2 * L + 3
+            for n in PREP_FIELDS:
+                if n == "tauref" and not prescribed:
+                    continue
+                shape = (ncol, lev + 1 if n == "tauref" else lev)
+                if dev:
+                    import torch
+                    out[n] = torch.empty(shape, dtype=torch.float64, device=st["t"].device)
+                else:
+                    out[n] = np.empty(shape)
+        keep: list = []
+        s = BatchState()
+        s.ncol, s.nlayers = ncol, L
+        s.device_ptrs = 1 if dev else 0
+        s.active_dust = 0 if prescribed else 1
+        s.cloudon = 1 if st.get("cloudon", 0) else 0
+        s.active_water = 1 if st.get("active_water", 0) else 0
+        s.ptrop = float(st["ptrop"])
+        s.psf = float(st.get("psf", 0.0))
+        s.rptau = float(st.get("rptau", 0.0))
+        s.mwratio = float(st.get("mwratio", 0.0))
+        for n in _ST_PTRS:
+            a = out.get(n) if n in PREP_FIELDS else st.get(n)
+            if a is not None and not dev and n not in PREP_FIELDS:
+                a = _host(a)
+            if a is not None:
+                keep.append(a)
+            setattr(s, n, _ptr(a))
+        bo = make_out(out)
+        rc = lib().mgcm_rt_run_state(self._h, C.byref(s), C.byref(bo))
+        if rc != 0:
+            raise RTError(rc, "mgcm_rt_run_state")
+        out["detau"], out["cumtauv"] = st["detau"], st["cumtauv"]
         return out
 
     # ---- captured uneven batches --------------------------------------

@@ -405,3 +405,47 @@ def make_tracer_batch(ncol: int, L: int = 24, seed: int = 0, active_dust: bool =
         t["ice_mass"] = t["ice_core_mass"] = t["ice_number"] = None
     t["meta"] = dict(b["meta"], tracers=True)
     return t
+
+
+def make_state_batch(ncol: int, L: int = 24, seed: int = 0, active_dust: bool = False,
+                     cloudon: bool = True, active_water: bool = True, vary_conr: bool = False,
+                     night_frac: float = 0.5, data_dir=None):
+    """Inputs of mgcm_rt_run_state: the GCM state of each column, before
+    COMP3 assembles the radiation arrays.  The columns of make_tracer_batch
+    (same seed) supply P(J,I), the tracers and the surface; from them:
+      t        TL(2l+2), the layer temperatures (the lapse-rate profile at
+               the layer mid-pressures), [ncol][L]
+      tstrat   the stratosphere temperature TL(2); gt the ground temperature
+      vapour   the water-vapour mass mixing ratio, uniform in the column
+      tautot   dust visible optical depth at RPTAU, lognormal(median 0.3,
+               sigma 0.6) (prescribed dust)
+      conr     the Conrath parameter: CONRNU (REAL*4 0.03,
+               code/modules.f90:874) or, with vary_conr, U[0.007, 0.04] (the
+               range of the latitude-varying form, code/dustprofile.f:106-114)
+    psf = 7.010 mbar (the tutorial namelist), RPTAU the module's REAL*4 6.1
+    (code/modules.f90:854), MWRATIO = MWCO2/MWH2O (code/input.f:180)."""
+    b = make_tracer_batch(ncol, L=L, seed=seed, active_dust=active_dust, cloudon=cloudon,
+                          night_frac=night_frac, data_dir=data_dir)
+    rng = np.random.default_rng(seed + 104729)
+    lev = 2 * L + 3
+    tlev = b["tlev"]
+    st = {k: b[k] for k in ("ncol", "L", "ptrop", "sigma", "sol", "pcol", "acosz", "als", "albi",
+                            "detau", "cumtauv", "dust_mass", "dust_number", "ice_mass",
+                            "ice_core_mass", "ice_number", "active_dust", "cloudon")}
+    st["t"] = np.ascontiguousarray(tlev[:, 3:lev - 1:2])      # K = 4, 6, .., 2L+2
+    st["tstrat"] = tlev[:, 0].copy()
+    st["gt"] = tlev[:, lev - 1].copy()
+    mwratio = MWCO2 / MWH2O
+    st["active_water"] = 1 if active_water else 0
+    st["mwratio"] = mwratio
+    st["vapour"] = np.repeat((b["qh2o"][:, 3] / mwratio)[:, None], L, axis=1) if active_water else None
+    st["psf"] = PSF_TUTORIAL
+    st["rptau"] = float(np.float32(RPTAU))
+    if not active_dust:
+        st["tautot"] = 0.3 * np.exp(0.6 * rng.standard_normal(ncol))
+        st["conr"] = (rng.uniform(0.007, 0.04, ncol) if vary_conr
+                      else np.full(ncol, float(np.float32(CONRNU))))
+    else:
+        st["tautot"] = st["conr"] = None
+    st["meta"] = dict(b["meta"], state=True, vary_conr=bool(vary_conr))
+    return st

@@ -1451,3 +1451,135 @@ static void aerosols_range(const orc_aero *a, const orc_tracers *t, int c0, int 
                         t->gicld + (size_t)c * 5 * lev1);
     }
 }
+
+/* ------------------------------------------------------------ column prep */
+
+/* code/dustprofile.f:100-104: REFPR = (5.0*PSF/PTROP)**(1.0/(FLOAT(NPDST)-1.0)),
+ * the exponent evaluated in REAL*4; PRDST(1) = PTROP, PRDST(n) = REFPR*PRDST(n-1). */
+void orc_dust_grid(double psf, double ptrop, double *prdst) {
+    const float e = 1.0f / ((float)ORC_NPDST - 1.0f);
+    const double refpr = mgcm_rt_pow(5.0 * psf / ptrop, (double)e);
+    prdst[0] = ptrop;
+    for (int n = 2; n <= ORC_NPDST; ++n) prdst[n - 1] = refpr * prdst[n - 2];
+}
+
+/* code/dustprofile.f:117-170 for one column: the normalising sum of the
+ * Conrath profile up to RPTAU, the mixing ratio QRDST per PRDST interval
+ * and its running integral TAUDST.  The literals 1. and 1.0 are exact. */
+void orc_dust_profile(const double *prdst, double rptau, double conr, double tautot, double *taudst) {
+#define PR(n) prdst[(n) - 1]
+    double sum = 0.0;
+    int n;
+    for (n = 2; n <= ORC_NPDST; ++n) {
+        if (PR(n) < rptau) {
+            const double pave = 0.5 * (PR(n) + PR(n - 1));
+            sum = sum + cexp_(conr * (1.0 - (rptau / pave))) * (PR(n) - PR(n - 1));
+        }
+        if (PR(n) >= rptau) break;
+    }
+    /* n = NPDST+1 when the loop ran to its end (code/dustprofile.f:132) */
+    {
+        const double pave = 0.5 * (rptau + PR(n - 1));
+        sum = sum + cexp_(conr * (1.0 - (rptau / pave))) * (rptau - PR(n - 1));
+    }
+    const double qrdst0 = tautot / sum;
+    double qrdst[ORC_NPDST];
+    for (n = 1; n <= ORC_NPDST - 1; ++n) {
+        qrdst[n - 1] = 0.0; /* every case below fails only for a NaN RPTAU */
+        if (rptau > PR(n + 1)) {
+            const double pave = 0.5 * (PR(n + 1) + PR(n));
+            qrdst[n - 1] = qrdst0 * cexp_(conr * (1.0 - (rptau / pave)));
+        }
+        if (rptau <= PR(n + 1) && rptau >= PR(n)) {
+            const double pave = 0.5 * (PR(n) + rptau);
+            const double pdif1 = rptau - PR(n), pdif2 = PR(n + 1) - rptau;
+            qrdst[n - 1] = qrdst0 * (cexp_(conr * (1.0 - (rptau / pave))) * pdif1 + pdif2) / (PR(n + 1) - PR(n));
+        }
+        if (rptau < PR(n)) qrdst[n - 1] = qrdst0;
+    }
+    taudst[0] = 0.0;
+    for (n = 2; n <= ORC_NPDST; ++n) taudst[n - 1] = taudst[n - 2] + qrdst[n - 2] * (PR(n) - PR(n - 1));
+#undef PR
+}
+
+/* code/jsrchgt.f90: index of the first SX(j) > TARGET by bisection. */
+int orc_jsrchgt(int n, const double *sx, double target) {
+    if (n < 1) return 0;
+    if (target > sx[n - 1]) return n + 1;
+    if (target < sx[0]) return 1;
+    int jl = 1, jh = n;
+    while (jh - jl > 1) {
+        const int jm = (jl + jh) / 2;
+        if (target > sx[jm - 1]) jl = jm;
+        else jh = jm;
+    }
+    if (target == sx[jh - 1]) jh = jh + 1;
+    return jh;
+}
+
+void orc_prep(const orc_prep_batch *b) {
+    const int L = b->L, lev = 2 * L + 3, lev1 = lev + 1;
+    double prdst[ORC_NPDST], taudst[ORC_NPDST], taucum[2 * ORC_MAXL + 4];
+    if (b->prescribed_dust) orc_dust_grid(b->psf, b->ptrop, prdst);
+    const double ptrop = b->ptrop;
+    const double *sig = b->sigma;
+    for (int c = 0; c < b->ncol; ++c) {
+        const double p = b->pcol[c];
+        const double *tl = b->t + (size_t)c * L;
+        double *plev = b->plev + (size_t)c * lev, *tlev = b->tlev + (size_t)c * lev;
+        double *pmid = b->pmid + (size_t)c * lev, *tmid = b->tmid + (size_t)c * lev;
+        double *qh = b->qh2o + (size_t)c * lev;
+        /* PL (code/potemp1.f:95-106) into PLEV (code/fillpt.f90:30-35) */
+        plev[0] = ptrop / 2.0;
+        plev[1] = ptrop / 2.0;
+        for (int k = 3; k <= lev - 1; ++k) plev[k - 1] = ptrop + sig[k - 1] * p;
+        plev[lev - 1] = ptrop + p;
+        /* TLEV (code/fillpt.f90:37-51): TSTRAT on 1-3, TL(2l+2) on the even
+         * levels, log-pressure interpolation on the odd ones, GT at the bottom */
+        for (int k = 1; k <= 3; ++k) tlev[k - 1] = b->tstrat[c];
+        for (int k = 4; k <= lev - 1; k += 2) tlev[k - 1] = tl[k / 2 - 2];
+        for (int k = 5; k <= lev - 2; k += 2)
+            tlev[k - 1] = tlev[k] + (tlev[k - 2] - tlev[k]) * mgcm_rt_ln(plev[k - 1] / plev[k]) /
+                                        mgcm_rt_ln(plev[k - 2] / plev[k]);
+        tlev[lev - 1] = b->gt[c];
+        /* TMID/PMID (code/fillpt.f90:53-70) */
+        tmid[0] = tlev[1];
+        tmid[1] = tlev[1];
+        pmid[0] = plev[0];
+        pmid[1] = plev[1];
+        for (int l = 1; l <= L; ++l) {
+            tmid[2 * l] = tlev[2 * l];
+            tmid[2 * l + 1] = tlev[2 * l];
+            pmid[2 * l] = plev[2 * l];
+            pmid[2 * l + 1] = plev[2 * l];
+        }
+        tmid[lev - 1] = tlev[lev - 1];
+        pmid[lev - 1] = plev[lev - 1];
+        /* QH2O (code/comp3.f:576-589) */
+        qh[0] = qh[1] = qh[2] = 0.0;
+        for (int l = 1; l <= L; ++l) {
+            const int k = 2 * l + 2;
+            qh[k - 1] = b->active_water ? b->mwratio * b->vapour[(size_t)c * L + l - 1] : R4(1.0E-7);
+            qh[k] = qh[k - 1];
+        }
+        if (!b->prescribed_dust) continue;
+        /* TAUREF (code/filltaucum.f:39-55, code/comp3.f:618) */
+        double *tr = b->tauref + (size_t)c * lev1;
+        orc_dust_profile(prdst, b->rptau, b->conr[c], b->tautot[c], taudst);
+        for (int k = 1; k <= 3; ++k) {
+            taucum[k - 1] = 0.0;
+            tr[k - 1] = 0.0;
+        }
+        for (int k = 4; k <= lev; ++k) {
+            const double pstar = p * sig[k - 1] + ptrop;
+            const double pstar1 = pstar > prdst[0] ? pstar : prdst[0];
+            int nstar = orc_jsrchgt(ORC_NPDST - 1, prdst, pstar1) - 1;
+            if (nstar > ORC_NPDST - 1) nstar = ORC_NPDST - 1;
+            if (nstar < 1) nstar = 1; /* PSTAR1 >= PRDST(1) gives nstar >= 1 (kept for NaN inputs) */
+            taucum[k - 1] = taudst[nstar - 1] + (pstar1 - prdst[nstar - 1]) * (taudst[nstar] - taudst[nstar - 1]) /
+                                                    (prdst[nstar] - prdst[nstar - 1]);
+            tr[k - 1] = taucum[k - 1] - taucum[k - 2];
+        }
+        tr[lev1 - 1] = 0.0;
+    }
+}

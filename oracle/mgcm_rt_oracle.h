@@ -146,6 +146,38 @@ void orc_aerosols_mt(const orc_aero *a, const orc_tracers *t, int nthreads);
 void orc_dsolflux(const orc_tables *t, int ncol, const double *sol, const double *acosz,
                   const double *detau, double *directsol);
 
+/* Column prep: the radiation's level inputs from the GCM state of a column.
+ *   PLEV/TLEV/PMID/TMID   PL of code/potemp1.f:95-106 through FILLPT
+ *                         (code/fillpt.f90:30-72); t[l] is TL(2l+2), the
+ *                         layer temperature after COLDAIR
+ *   QH2O                  code/comp3.f:576-589 (MWRATIO * vapour, or the
+ *                         REAL*4 1.0E-7 without active water); levels 1-3
+ *                         are not set by COMP3 and are 0 here
+ *   TAUREF (prescribed)   the Conrath profile of code/dustprofile.f:88-172
+ *                         on the PRDST grid, sampled by FILLTAUCUM
+ *                         (code/filltaucum.f:39-55, JSRCHGT of
+ *                         code/jsrchgt.f90)
+ * Per-column inputs [ncol] or [ncol][L]; outputs as in orc_batch. */
+#define ORC_NPDST 100
+typedef struct {
+    int ncol, L, active_water, prescribed_dust;
+    double ptrop, psf, rptau, mwratio;
+    const double *sigma;                    /* [2L+3] */
+    const double *pcol, *tstrat, *gt;       /* [ncol] P(J,I), TSTRAT, GT */
+    const double *t;                        /* [ncol][L] */
+    const double *vapour;                   /* [ncol][L] (active_water) */
+    const double *tautot, *conr;            /* [ncol] (prescribed_dust) */
+    double *plev, *tlev, *pmid, *tmid, *qh2o; /* [ncol][2L+3] */
+    double *tauref;                         /* [ncol][2L+4] (prescribed_dust) */
+} orc_prep_batch;
+/* PRDST(1..NPDST) of code/dustprofile.f:100-104. */
+void orc_dust_grid(double psf, double ptrop, double *prdst);
+/* TAUDST(J,I,1..NPDST) of one column (code/dustprofile.f:117-170). */
+void orc_dust_profile(const double *prdst, double rptau, double conr, double tautot, double *taudst);
+/* JSRCHGT (code/jsrchgt.f90), 1-based result. */
+int orc_jsrchgt(int n, const double *sx, double target);
+void orc_prep(const orc_prep_batch *b);
+
 #ifdef __cplusplus
 }
 #endif

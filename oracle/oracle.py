@@ -249,3 +249,86 @@ def aerosols(aero: AeroTables, tb: dict, nthreads: int = 1) -> dict:
     for k in ("dust_mass", "dust_number", "ice_mass", "ice_core_mass", "ice_number", "active_dust", "cloudon"):
         out.pop(k, None)
     return out
+
+
+# ---- column prep (code/potemp1.f, fillpt.f90, comp3.f:576-589, dustprofile.f, filltaucum.f)
+NPDST = 100
+
+
+class OrcPrep(C.Structure):
+    _fields_ = [("ncol", C.c_int), ("L", C.c_int), ("active_water", C.c_int), ("prescribed_dust", C.c_int),
+                ("ptrop", C.c_double), ("psf", C.c_double), ("rptau", C.c_double), ("mwratio", C.c_double)] + [
+        (n, C.c_void_p) for n in ("sigma", "pcol", "tstrat", "gt", "t", "vapour", "tautot", "conr",
+                                  "plev", "tlev", "pmid", "tmid", "qh2o", "tauref")]
+
+
+def _prep_lib(variant: str = "rt"):
+    L = lib(variant)
+    L.orc_prep.argtypes = [C.POINTER(OrcPrep)]
+    L.orc_dust_grid.argtypes = [C.c_double, C.c_double, _D]
+    L.orc_dust_profile.argtypes = [_D, C.c_double, C.c_double, C.c_double, _D]
+    L.orc_jsrchgt.argtypes = [C.c_int, _D, C.c_double]
+    L.orc_jsrchgt.restype = C.c_int
+    return L
+
+
+def dust_grid(psf: float, ptrop: float) -> np.ndarray:
+    """PRDST(1..NPDST) (code/dustprofile.f:100-104)."""
+    out = np.empty(NPDST)
+    _prep_lib().orc_dust_grid(psf, ptrop, _p(out))
+    return out
+
+
+def dust_profile(prdst, rptau: float, conr: float, tautot: float) -> np.ndarray:
+    """TAUDST(1..NPDST) of one column (code/dustprofile.f:117-170)."""
+    pr = np.ascontiguousarray(prdst, dtype=np.float64)
+    out = np.empty(NPDST)
+    _prep_lib().orc_dust_profile(_p(pr), rptau, conr, tautot, _p(out))
+    return out
+
+
+def jsrchgt(sx, target: float) -> int:
+    """JSRCHGT(N, SX, 1, TARGET) (code/jsrchgt.f90), 1-based."""
+    a = np.ascontiguousarray(sx, dtype=np.float64)
+    return int(_prep_lib().orc_jsrchgt(len(a), _p(a), target))
+
+
+def prep(st: dict) -> dict:
+    """State batch (synth.make_state_batch) -> the tracer batch COMP3 would
+    hand to the aerosol optics: PLEV/TLEV/PMID/TMID/QH2O, and TAUREF for
+    prescribed dust, filled as the reference fills them."""
+    ncol, L = int(st["ncol"]), int(st["L"])
+    lev = 2 * L + 3
+    prescribed = not st.get("active_dust", 0)
+    water = bool(st.get("active_water", 0))
+    keep = []
+    def inp(k):
+        v = st.get(k)
+        if v is None:
+            return None
+        v = np.ascontiguousarray(v, dtype=np.float64)
+        keep.append(v)
+        return v.ctypes.data
+    out = {n: np.zeros((ncol, lev)) for n in ("plev", "tlev", "pmid", "tmid", "qh2o")}
+    out["tauref"] = np.zeros((ncol, lev + 1)) if prescribed else None
+    s = OrcPrep()
+    s.ncol, s.L = ncol, L
+    s.active_water = 1 if water else 0
+    s.prescribed_dust = 1 if prescribed else 0
+    s.ptrop = float(st["ptrop"])
+    s.psf = float(st.get("psf", 0.0))
+    s.rptau = float(st.get("rptau", 0.0))
+    s.mwratio = float(st.get("mwratio", 0.0))
+    for k in ("sigma", "pcol", "tstrat", "gt", "t"):
+        setattr(s, k, inp(k))
+    s.vapour = inp("vapour") if water else None
+    s.tautot = inp("tautot") if prescribed else None
+    s.conr = inp("conr") if prescribed else None
+    for k, v in out.items():
+        setattr(s, k, v.ctypes.data if v is not None else None)
+    _prep_lib().orc_prep(C.byref(s))
+    tb = {k: st[k] for k in ("ncol", "L", "ptrop", "sigma", "sol", "pcol", "acosz", "als", "albi",
+                             "detau", "cumtauv", "dust_mass", "dust_number", "ice_mass", "ice_core_mass",
+                             "ice_number", "active_dust", "cloudon")}
+    tb.update(out)
+    return tb
