@@ -17,9 +17,11 @@ struct Lay {   // per-layer two-stream coefficients
     double gama, e1, e2, e3, e4, cp, cm, cpm1, cmm1;
 };
 
-// Per-system arrays (1-based layer index).  Pass A fills a0..a4; pass C
-// writes the layer's two-stream coefficients over the pass-A slots it has
-// consumed (plus c5), and the DSOLVER rows' AS/DS for the back-substitution.
+// Per-system arrays (1-based layer index).  Pass A fills a0..a4; the visible
+// pass C writes the layer's two-stream coefficients over the pass-A slots it
+// has consumed (plus c5) -- the IR passes C and D recompute theirs from the
+// pass-A slots instead -- and both write the DSOLVER rows' AS/DS for the
+// back-substitution.
 struct SysLocal {
     double a0[D_MAXNL + 1], a1[D_MAXNL + 1], a2[D_MAXNL + 1], a3[D_MAXNL + 2], a4[D_MAXNL + 1];
     double c5[D_MAXNL + 1];
@@ -404,17 +406,25 @@ __device__ void solve_ir(const SegDev &sg, int c, int nw, int ng, int sidx, ColS
     const double tautop = w.a2[1] * plev[2 - 1] / (plev[4 - 1] - plev[2 - 1]);
     const double btop = (1.0 - mgcm_rt_exp(-tautop / UBARI)) * s.pltop_i[nw - 1];
     const double bsurf = s.bsurf_i[nw - 1];
-    // LAMDA -> a0 (over WBARI), GAMA -> a1, B1 -> c5, TERM -> a3 (a1, a3 unused by pass A)
-    double *LAM = w.a0, *GAM = w.a1, *B1 = w.c5, *TERM = w.a3;
-    auto coef = [&](int l, double w0, double dt) {
-        Lay y;
+    // LAMDA, GAMA, B1, TERM of layer l (code/gfluxi.f90:219-240).  Pass C
+    // and pass D both evaluate them from the pass-A slots (WBARI, DTAUI),
+    // which stay intact: recomputing costs less than a round trip of four
+    // more per-layer arrays through local memory (measured on the c1 call:
+    // 15.8 -> 15.4 ms).  The visible solve keeps its stored coefficients:
+    // there the recomputation measured slower.
+    auto lay4 = [&](int l, double w0, double dt, double &lam, double &gama, double &b1, double &term) {
         const double cb = s.cosb_i[l * D_NI + nw - 1];
         const double alpha = sqrt((1.0 - w0) / (1.0 - w0 * cb));
-        const double lam = alpha * (1.0 - w0 * cb) / UBARI;
+        lam = alpha * (1.0 - w0 * cb) / UBARI;
+        b1 = s.pdif_i[l * D_NI + nw - 1] / dt;
+        gama = (1.0 - alpha) / (1.0 + alpha);
+        term = UBARI / (1.0 - w0 * cb);
+    };
+    auto coef = [&](int l, double w0, double dt) {
+        Lay y;
+        double lam, b1, term;
+        lay4(l, w0, dt, lam, y.gama, b1, term);
         const double b0 = s.b0_i[l * D_NI + nw - 1];
-        const double b1 = s.pdif_i[l * D_NI + nw - 1] / dt;
-        y.gama = (1.0 - alpha) / (1.0 + alpha);
-        const double term = UBARI / (1.0 - w0 * cb);
         y.cp = b0 + b1 * dt + b1 * term;
         y.cm = b0 + b1 * dt - b1 * term;
         y.cpm1 = b0 + b1 * term;
@@ -425,10 +435,6 @@ __device__ void solve_ir(const SegDev &sg, int c, int nw, int ng, int sidx, ColS
         y.e2 = ep - y.gama * em;
         y.e3 = y.gama * ep + em;
         y.e4 = y.gama * ep - em;
-        LAM[l] = lam;
-        GAM[l] = y.gama;
-        B1[l] = b1;
-        TERM[l] = term;
         return y;
     };
     double pw0 = w.a0[NL - 1], pdt = w.a2[NL - 1];
@@ -449,22 +455,22 @@ __device__ void solve_ir(const SegDev &sg, int c, int nw, int ng, int sidx, ColS
 
     double xprev = 0.0;
     double nas1 = w.as[1], nds1 = w.ds[1], nas2 = w.as[2], nds2 = w.ds[2];
-    double nlam = LAM[1], ngam = GAM[1], nb1 = B1[1], nterm = TERM[1];
+    double nw0 = w.a0[1], ndt = w.a2[1];
     double ndtk = 1 < NL ? w.a4[1] : w.a2[1];
     for (int n = 1; n <= NL; ++n) {
         const double as1 = nas1, ds1 = nds1, as2 = nas2, ds2 = nds2;
-        const double lam = nlam, gama = ngam, b1 = nb1, term = nterm, dtk = ndtk;
+        const double dtk = ndtk, w0n = nw0, dtn = ndt;
         if (n < NL) {
             nas1 = w.as[2 * n + 1];
             nds1 = w.ds[2 * n + 1];
             nas2 = w.as[2 * n + 2];
             nds2 = w.ds[2 * n + 2];
-            nlam = LAM[n + 1];
-            ngam = GAM[n + 1];
-            nb1 = B1[n + 1];
-            nterm = TERM[n + 1];
+            nw0 = w.a0[n + 1];
+            ndt = w.a2[n + 1];
             ndtk = n + 1 < NL ? w.a4[n + 1] : w.a2[n + 1];
         }
+        double lam, gama, b1, term;
+        lay4(n, w0n, dtn, lam, gama, b1, term);
         const double xa = n == 1 ? ds1 : ds1 - as1 * xprev;
         const double xb = ds2 - as2 * xa;
         xprev = xb;
