@@ -1036,9 +1036,10 @@ int issue_tracer_job(mgcm_rt_handle *h, Slot &sl, cudaStream_t st, const mgcm_rt
         rt_prep<<<pg, PREP_THREADS, 0, st>>>(ps);
         CK(cudaGetLastError());
     }
-    const long long items = (long long)n * (L + 1);
-    const int ag = (int)std::min<long long>((items + 127) / 128, (long long)h->num_sms * 16);
-    rt_aerosol<<<ag, 128, 0, st>>>(as, h->aero, h->d_mie);
+    // a warp per column, AERO_WARPS columns per CTA, up to 8 CTAs per SM resident
+    const int ag = (int)std::min<long long>(((long long)n + AERO_WARPS - 1) / AERO_WARPS,
+                                            (long long)h->num_sms * 8);
+    rt_aerosol<<<ag, 32 * AERO_WARPS, 0, st>>>(as, h->aero, h->d_mie);
     CK(cudaGetLastError());
     rc = launch_all(h, sl, st, (int)n, nl, 1 << 30);
     if (rc) return rc;

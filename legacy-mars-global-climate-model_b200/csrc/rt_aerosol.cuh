@@ -28,6 +28,7 @@ struct AeroSeg {
     double *taurefcld, *qextrefcld, *qxvcld, *qsvcld, *gvcld, *qxicld, *qsicld, *gicld;
 };
 
+constexpr int AERO_WARPS = 4;   // columns (warps) per CTA of rt_aerosol
 __global__ void rt_aerosol(const AeroSeg a, const AeroConst K, const double *__restrict__ mie);
 
 }  // namespace mgcm
