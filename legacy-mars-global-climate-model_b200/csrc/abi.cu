@@ -92,6 +92,10 @@ namespace {
 
 constexpr int BLOCK = 224;
 constexpr int SYNC_JOB_COLS = 8192;     // columns per job of a synchronous host-buffer call (measured best of 2k-32k)
+#ifndef MGCM_SYNC_RAMP
+#define MGCM_SYNC_RAMP 2048
+#endif
+constexpr int SYNC_RAMP_COLS = MGCM_SYNC_RAMP;   // first (and last) job of a ramped host-buffer call
 constexpr int SERVE_JOB_COLS = 32768;   // columns per job of a served request
 constexpr int SERVE_SLOTS = 4;          // serving slots at most
 
@@ -722,6 +726,30 @@ int finish_pending(mgcm_rt_handle *h) {
     return status_to_code(*sl.h_status);
 }
 
+// Column ranges (ends) of a synchronous host-buffer call over n columns: jobs
+// of up to max_job columns.  With first > 0 the jobs ramp up (first, 2 first,
+// ... below max_job) and back down at the end, so the first host-to-device
+// copy and the last device-to-host copy, which no kernel overlaps, are short;
+// the middle is split evenly.
+std::vector<int> job_ends(int n, int max_job, int first) {
+    std::vector<int> ramp, ends;
+    int ramp_cols = 0;
+    for (int sz = first; first > 0 && sz < max_job; sz *= 2) {
+        ramp.push_back(sz);
+        ramp_cols += sz;
+    }
+    int c = 0;
+    if (!ramp.empty() && n >= 2 * ramp_cols + max_job) {
+        for (int sz : ramp) ends.push_back(c += sz);
+        const int mid = n - 2 * ramp_cols, nj = (mid + max_job - 1) / max_job;
+        for (int j = 0; j < nj; ++j) ends.push_back(c += mid / nj + (j < mid % nj ? 1 : 0));
+        for (auto it = ramp.rbegin(); it != ramp.rend(); ++it) ends.push_back(c += *it);
+    } else {
+        while (c < n) ends.push_back(c = std::min(n, c + max_job));
+    }
+    return ends;
+}
+
 // Synchronous batch of host-pointer segments: jobs alternate between the two
 // synchronous slots, forked from and joined back into the caller's stream.
 int run_host(mgcm_rt_handle *h, int nbatch, const mgcm_rt_batch_in *in, mgcm_rt_batch_out *out) {
@@ -734,8 +762,8 @@ int run_host(mgcm_rt_handle *h, int nbatch, const mgcm_rt_batch_in *in, mgcm_rt_
     bool used[2] = {false, false};
     for (int b = 0; b < nbatch; ++b) {
         const Sizes z = sizes_of(in[b]);
-        for (int c0 = 0; c0 < (int)z.ncol; c0 += SYNC_JOB_COLS, ++k) {
-            const int c1 = std::min((int)z.ncol, c0 + SYNC_JOB_COLS);
+        int c0 = 0;
+        for (const int c1 : job_ends((int)z.ncol, SYNC_JOB_COLS, SYNC_RAMP_COLS)) {
             Slot &sl = *h->slots[k & 1];
             if (used[k & 1]) {   // the slot's previous job must finish before its buffers are reused
                 CK(cudaEventSynchronize(sl.done));
@@ -747,6 +775,8 @@ int run_host(mgcm_rt_handle *h, int nbatch, const mgcm_rt_batch_in *in, mgcm_rt_
             used[k & 1] = true;
             nk += sl.kernels;
             cols += c1 - c0;
+            c0 = c1;
+            ++k;
         }
     }
     for (int i = 0; i < 2; ++i) {
@@ -1066,9 +1096,10 @@ int run_tracers(mgcm_rt_handle *h, const mgcm_rt_batch_tracers &in, mgcm_rt_batc
     long long systems = 0;
     int nk = 0, k = 0;
     bool used[2] = {false, false};
-    const int job = in.device_ptrs ? 4 * SYNC_JOB_COLS : SYNC_JOB_COLS;
-    for (int c0 = 0; c0 < in.ncol; c0 += job, ++k) {
-        const int c1 = std::min(in.ncol, c0 + job);
+    const std::vector<int> ends = in.device_ptrs ? job_ends(in.ncol, 4 * SYNC_JOB_COLS, 0)
+                                                 : job_ends(in.ncol, SYNC_JOB_COLS, SYNC_RAMP_COLS);
+    int c0 = 0;
+    for (const int c1 : ends) {
         Slot &sl = *h->slots[k & 1];
         if (used[k & 1]) {
             CK(cudaEventSynchronize(sl.done));
@@ -1079,6 +1110,8 @@ int run_tracers(mgcm_rt_handle *h, const mgcm_rt_batch_tracers &in, mgcm_rt_batc
         if (rc) return rc;
         used[k & 1] = true;
         nk += sl.kernels;
+        c0 = c1;
+        ++k;
     }
     for (int i = 0; i < 2; ++i) {
         Slot &sl = *h->slots[i];
