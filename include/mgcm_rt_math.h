@@ -61,11 +61,13 @@ static const double mgcm_rt_exp_tab_host[64] = MGCM_RT_EXP_TABLE;
 #define MGCM_RT_ADD(a, b) __dadd_rn((a), (b))
 #define MGCM_RT_RINT(x) rint(x)
 #define MGCM_RT_TAB(i) __ldg(&mgcm_rt_exp_tab_dev[i])
+#define MGCM_RT_UNROLL _Pragma("unroll")
 #else
 #define MGCM_RT_MUL(a, b) ((a) * (b))
 #define MGCM_RT_ADD(a, b) ((a) + (b))
 #define MGCM_RT_RINT(x) nearbyint(x)
 #define MGCM_RT_TAB(i) (mgcm_rt_exp_tab_host[i])
+#define MGCM_RT_UNROLL
 #endif
 
 MGCM_RT_HD double mgcm_rt_pow2i(int m) {
@@ -199,12 +201,17 @@ MGCM_RT_HD double mgcm_rt_pow(double x, double y) {
 /* Error function (the DERF of the aerosol size-bin weights,
  * code/opt_dst.f:120-121).  |x| < 1.5: Maclaurin series
  *   erf x = 2/sqrt(pi) sum_n (-1)^n x^(2n+1) / (n! (2n+1)),
- * summed until the terms fall below 2^-60 of the sum (at most 60 terms);
+ * each term the previous one times -x^2 times the reciprocals 1/n and
+ * 1/(2n+1) (correctly rounded: constants once the device unrolls the loop,
+ * a division on the host), summed until the terms fall below 2^-60 of the
+ * sum (at most 60 terms, 26 below 1.5);
  * 1.5 <= |x| < 6: erf x = 1 - erfc x with the continued fraction
  *   erfc x = exp(-x^2)/sqrt(pi) / (x + (1/2)/(x + 1/(x + (3/2)/(x + ...)))),
- * its 100th convergent A/B from the forward three-term recurrences
- * (A, B stay below 1e100 on this range); |x| >= 6: +-1.
- * Absolute error below 1e-15; identical on host and device. */
+ * its 80th convergent A/B from the forward three-term recurrences (A, B stay
+ * below 1e100 on this range; 80 terms converge to 1e-16 from x = 1.5 on);
+ * |x| >= 6: +-1.  Absolute error below 1e-15 (8.9e-16 at most over a
+ * 140,001-point scan of [-7, 7] against libm); identical on host and
+ * device. */
 MGCM_RT_HD double mgcm_rt_erf(double x) {
     const double TWO_RSQPI = 0x1.20dd750429b6dp+0, RSQPI = 0x1.20dd750429b6dp-1;
     const double ax = x < 0.0 ? -x : x;
@@ -212,9 +219,10 @@ MGCM_RT_HD double mgcm_rt_erf(double x) {
     if (ax < 1.5) {
         const double mx2 = -MGCM_RT_MUL(x, x);
         double t = x, sum = x;
+        MGCM_RT_UNROLL
         for (int n = 1; n <= 60; ++n) {
-            t = MGCM_RT_MUL(t, mx2) / (double)n;
-            const double term = t / (double)(2 * n + 1);
+            t = MGCM_RT_MUL(MGCM_RT_MUL(t, mx2), 1.0 / (double)n);
+            const double term = MGCM_RT_MUL(t, 1.0 / (double)(2 * n + 1));
             sum = MGCM_RT_ADD(sum, term);
             const double at = term < 0.0 ? -term : term, as = sum < 0.0 ? -sum : sum;
             if (at < MGCM_RT_MUL(as, 0x1.0p-60)) break;
@@ -225,7 +233,8 @@ MGCM_RT_HD double mgcm_rt_erf(double x) {
         r = 1.0;
     } else {
         double a1 = 1.0, a0 = ax, b1 = 0.0, b0 = 1.0;
-        for (int n = 1; n <= 100; ++n) {
+        MGCM_RT_UNROLL
+        for (int n = 1; n <= 80; ++n) {
             const double an = MGCM_RT_MUL(0.5, (double)n);
             const double a = MGCM_RT_ADD(MGCM_RT_MUL(ax, a0), MGCM_RT_MUL(an, a1));
             const double b = MGCM_RT_ADD(MGCM_RT_MUL(ax, b0), MGCM_RT_MUL(an, b1));
