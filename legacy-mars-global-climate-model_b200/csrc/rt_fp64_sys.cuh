@@ -106,18 +106,22 @@ __device__ __forceinline__ void unmix(double xa, double xb, double &xk1, double 
     if (xk2 != 0.0 && fabs(xk2 / (xa + R4(1.e-20))) < R4(1.E-30)) xk2 = 0.0;
 }
 
+// Table strides of the k-table corners: MP+1 and MT+1 (elements).
+constexpr int KT_DP = D_NH * D_NGK, KT_DT = D_NP * D_NH * D_NGK;
+
 // 8-corner gather and interpolation (optcv.f90:279-301): returns TAUGAS.
+// tb points at the band's table plus the Gauss point; the level's corner
+// offset and NH2O step come staged (ColSmem::kofs, kdh).
 __device__ __forceinline__ double taugas_at(const ColSmem &s, int k, const double *__restrict__ tb) {
-    const int mt = s.mt[k] - 1, mp = s.mp[k] - 1, nh = s.nh[k] - 1;
-    const int nh1 = nh + 1 < D_NH ? nh + 1 : D_NH - 1;   // WRATIO = 0 when NH2O = 10
+    const double *p = tb + s.kofs[k];
+    const int dh = s.kdh[k];
     const double wr = s.wr[k];
-    auto corner = [&](int a, int b) {
-        const double *p = tb + ((size_t)(a * D_NP + b) * D_NH) * D_NGK;
-        const double c0 = __ldg(p + nh * D_NGK), c1 = __ldg(p + nh1 * D_NGK);
+    auto corner = [&](int off) {
+        const double c0 = __ldg(p + off), c1 = __ldg(p + off + dh);
         return c0 + wr * (c1 - c0);
     };
-    const double k1 = corner(mt, mp), k2 = corner(mt, mp + 1);
-    const double k3 = corner(mt + 1, mp + 1), k4 = corner(mt + 1, mp);
+    const double k1 = corner(0), k2 = corner(KT_DP);
+    const double k3 = corner(KT_DT + KT_DP), k4 = corner(KT_DT);
     const double ans = s.lk[4 * k] * k1 + s.lk[4 * k + 1] * k2 + s.lk[4 * k + 2] * k3 + s.lk[4 * k + 3] * k4;
     return s.u[k] * ans;
 }
@@ -125,16 +129,15 @@ __device__ __forceinline__ double taugas_at(const ColSmem &s, int k, const doubl
 
 // TAUGAS at level k from the FP32 table of Cmk*k (mixed precision).
 __device__ __forceinline__ float taugas_f(const ColSmem &s, int k, const float *__restrict__ tb) {
-    const int mt = s.mt[k] - 1, mp = s.mp[k] - 1, nh = s.nh[k] - 1;
-    const int nh1 = nh + 1 < D_NH ? nh + 1 : D_NH - 1;
+    const float *p = tb + s.kofs[k];
+    const int dh = s.kdh[k];
     const float wr = (float)s.wr[k];
-    auto corner = [&](int a, int b) {
-        const float *p = tb + ((size_t)(a * D_NP + b) * D_NH) * D_NGK;
-        const float c0 = __ldg(p + nh * D_NGK), c1 = __ldg(p + nh1 * D_NGK);
+    auto corner = [&](int off) {
+        const float c0 = __ldg(p + off), c1 = __ldg(p + off + dh);
         return c0 + wr * (c1 - c0);
     };
-    const float k1 = corner(mt, mp), k2 = corner(mt, mp + 1);
-    const float k3 = corner(mt + 1, mp + 1), k4 = corner(mt + 1, mp);
+    const float k1 = corner(0), k2 = corner(KT_DP);
+    const float k3 = corner(KT_DT + KT_DP), k4 = corner(KT_DT);
     const float ans = (float)s.lk[4 * k] * k1 + (float)s.lk[4 * k + 1] * k2 +
                       (float)s.lk[4 * k + 2] * k3 + (float)s.lk[4 * k + 3] * k4;
     return (float)s.dpr[k] * ans;
@@ -341,6 +344,11 @@ __device__ void solve_vis(const SegDev &sg, int c, int nw, int ng, int sidx, Col
 }
 
 // ---------------------------------------------------------------- infrared
+#ifndef MGCM_IR_SCREEN_UNROLL
+#define MGCM_IR_SCREEN_UNROLL 2
+#endif
+constexpr int IR_SCREEN_UNROLL = MGCM_IR_SCREEN_UNROLL;
+
 template <int MODE>
 __device__ void solve_ir(const SegDev &sg, int c, int nw, int ng, int sidx, ColSmem &s,
                          const RtConst &K, const double *__restrict__ ki, SysLocal &w,
@@ -362,6 +370,31 @@ __device__ void solve_ir(const SegDev &sg, int c, int nw, int ng, int sidx, ColS
         }
         return ta + tcl;
     };
+    if (MODE == 1) {
+        // The screen needs TAUGSURF only: the gas optical depths of levels
+        // 2..LEV summed in order (code/optci.f90:143-167).  The gathers of
+        // IR_SCREEN_UNROLL levels are issued before they are summed, so a
+        // warp has that many levels' table reads in flight.
+        double taug = 0.0;
+        if (ng < D_NG) {
+            int k = 2;
+            for (; k + IR_SCREEN_UNROLL - 1 <= LEV; k += IR_SCREEN_UNROLL) {
+                double tg[IR_SCREEN_UNROLL];
+#pragma unroll
+                for (int u = 0; u < IR_SCREEN_UNROLL; ++u) tg[u] = taugas_at(s, k + u, tb);
+#pragma unroll
+                for (int u = 0; u < IR_SCREEN_UNROLL; ++u) taug += tg[u];
+            }
+            for (; k <= LEV; ++k) taug += taugas_at(s, k, tb);
+            if (taug < TLIMITI) {
+                s.skip[sidx] = 1;
+                return;
+            }
+        }
+        s.skip[sidx] = 0;
+        ++nsolved;
+        return;
+    }
     // pass A. a0 = WBARI, a1 = COSBI, a2 = DTAUI, a4 = TAUCUMI(2l+1)-TAUCUMI(2l)
     const double tiny = R4(1.0E-9);
     double tc = 0.0 + dtauk(2);

@@ -27,9 +27,9 @@ __device__ inline void stage_level(const SegDev &sg, int c, const RtConst &K, Co
             int mt, mp, nh;
             double wr, lk[4];
             tpindex_dev(K, pmid[k - 1], tmid[k - 1], qh2o[k - 1], mt, mp, nh, wr, lk);
-            s.mt[k] = mt;
-            s.mp[k] = mp;
-            s.nh[k] = nh;
+            const int nh1 = nh < D_NH ? nh + 1 : D_NH;   // WRATIO = 0 when NH2O = 10
+            s.kofs[k] = (((mt - 1) * D_NP + (mp - 1)) * D_NH + (nh - 1)) * D_NGK;
+            s.kdh[k] = (nh1 - nh) * D_NGK;
             s.wr[k] = wr;
             s.lk[4 * k + 0] = lk[0];
             s.lk[4 * k + 1] = lk[1];
