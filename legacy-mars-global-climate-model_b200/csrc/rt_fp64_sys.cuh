@@ -100,10 +100,15 @@ __device__ __forceinline__ void top_row(const Lay &t, double btop, SysLocal &w, 
 }
 
 // XK(2n-1), XK(2n) -> XK1, XK2 with the underflow test of dsolver.f90:91-101.
+// The test divides; when |XK2| >= 2e-30 |XA + 1e-20| (the usual case) the
+// quotient is above the REAL*4 1E-30 whatever its rounding, so the division
+// is skipped.  Zero, infinite and NaN operands fail that comparison and take
+// the reference's division.
 __device__ __forceinline__ void unmix(double xa, double xb, double &xk1, double &xk2) {
     xk1 = xa + xb;
     xk2 = xa - xb;
-    if (xk2 != 0.0 && fabs(xk2 / (xa + R4(1.e-20))) < R4(1.E-30)) xk2 = 0.0;
+    const double d = xa + R4(1.e-20);
+    if (xk2 != 0.0 && !(fabs(xk2) >= 2.0e-30 * fabs(d)) && fabs(xk2 / d) < R4(1.E-30)) xk2 = 0.0;
 }
 
 // Table strides of the k-table corners: MP+1 and MT+1 (elements).
