@@ -39,7 +39,7 @@ def _state(ncol, L, seed, case):
 
 
 @pytest.mark.parametrize("case", CASES)
-@pytest.mark.parametrize("L", [24, 36])
+@pytest.mark.parametrize("L", [24, 36, 48])
 def test_state_prep_bit_exact_and_fp64_parity(data_dir, otables, aero, case, L):
     st = _state(193, L, 700 + L + 7 * CASES.index(case), case)
     tb = oracle.prep(st)
@@ -73,13 +73,18 @@ def test_state_equals_tracers_on_prepared_arrays(data_dir):
         rt.close()
 
 
-def test_state_mixed_within_tolerance(data_dir, otables, aero):
-    st = _state(512, 24, 761, CASES[0])
+@pytest.mark.parametrize("case", [CASES[0], CASES[2]])
+def test_state_mixed_within_tolerance(data_dir, otables, aero, case):
+    st = _state(512, 24, 761 + CASES.index(case), case)
     tb = oracle.prep(st)
     ref = oracle.run_batch(otables, oracle.aerosols(aero, tb))
     rt = abi.Radiation(data_dir, max_layers=24, precision=abi.MIXED, validate=True)
     try:
-        err = mixed_errors(tb, rt.run_state(st), ref)
+        got = rt.run_state(st, return_levels=True)
+        for k in abi.PREP_FIELDS:   # the prep is FP64 in both modes
+            if tb[k] is not None:
+                np.testing.assert_array_equal(got[k], tb[k], err_msg=k)
+        err = mixed_errors(tb, got, ref)
         assert err["flux_max"] <= 1e-3 and err["heat_dT_Ksol_max"] <= 1e-2, err
     finally:
         rt.close()
