@@ -117,7 +117,7 @@ __global__ void validate_kernel(const SegTable *__restrict__ st, uint32_t *statu
         fin(sg.pmid + (size_t)c * LEV, LEV);
         fin(sg.tmid + (size_t)c * LEV, LEV);
         fin(sg.qh2o + (size_t)c * LEV, LEV);
-        fin(sg.tauref + (size_t)c * LEV1, LEV1);
+        fin(sg.tauref + (size_t)c * LEV1, sg.dust_band ? LEV : LEV1);   // TAUREF(LEV+1) is 0 then
         fin(sg.qextrefdst + (size_t)c * LEV1, LEV1);
         fin(sg.qxvdst + (size_t)c * 7 * LEV1, 7 * LEV1);
         fin(sg.qsvdst + (size_t)c * 7 * LEV1, 7 * LEV1);
@@ -998,9 +998,11 @@ int issue_tracer_job(mgcm_rt_handle *h, Slot &sl, cudaStream_t st, const mgcm_rt
     }
     // the per-level aerosol arrays of the ABI, on the device (+ the prepared
     // level arrays of a state batch that the caller does not take)
+    // (prescribed dust needs no per-level arrays: the stage reads the band
+    // constants, SegDev::dust_band, and TAUREF as given)
     const size_t per = (size_t)lev1 * (2 + 3 * (AERO_NV + AERO_NI));
     const size_t prep_per = stt ? (size_t)5 * lev + lev1 : 0;
-    const size_t abytes = n * (per * (in.cloudon ? 2 : 1) + prep_per) * 8;
+    const size_t abytes = n * (per * ((in.active_dust ? 1 : 0) + (in.cloudon ? 1 : 0)) + prep_per) * 8;
     int rc = arena_ensure(h, sl.aero, abytes, st);
     if (rc) return rc;
     double *ap = static_cast<double *>(sl.aero.ptr);
@@ -1019,14 +1021,16 @@ int issue_tracer_job(mgcm_rt_handle *h, Slot &sl, cudaStream_t st, const mgcm_rt
         ps.qh2o = const_cast<double *>(sd.qh2o);
         ps.tauref = const_cast<double *>(as.tauref_in);
     }
-    as.tauref = take(lev1);
-    as.qextrefdst = take(lev1);
-    as.qxvdst = take((size_t)AERO_NV * lev1);
-    as.qsvdst = take((size_t)AERO_NV * lev1);
-    as.gvdst = take((size_t)AERO_NV * lev1);
-    as.qxidst = take((size_t)AERO_NI * lev1);
-    as.qsidst = take((size_t)AERO_NI * lev1);
-    as.gidst = take((size_t)AERO_NI * lev1);
+    if (in.active_dust) {
+        as.tauref = take(lev1);
+        as.qextrefdst = take(lev1);
+        as.qxvdst = take((size_t)AERO_NV * lev1);
+        as.qsvdst = take((size_t)AERO_NV * lev1);
+        as.gvdst = take((size_t)AERO_NV * lev1);
+        as.qxidst = take((size_t)AERO_NI * lev1);
+        as.qsidst = take((size_t)AERO_NI * lev1);
+        as.gidst = take((size_t)AERO_NI * lev1);
+    }
     if (in.cloudon) {
         as.taurefcld = take(lev1);
         as.qextrefcld = take(lev1);
@@ -1038,7 +1042,11 @@ int issue_tracer_job(mgcm_rt_handle *h, Slot &sl, cudaStream_t st, const mgcm_rt
         as.gicld = take((size_t)AERO_NI * lev1);
     }
     as.plev = sd.plev;
-    sd.tauref = as.tauref;
+    if (!in.active_dust) {
+        sd.dust_band = h->d_mie + AERO_MIE_SIZE;
+        as.tauref = nullptr;   // rt_aerosol leaves the dust alone
+    }
+    sd.tauref = in.active_dust ? as.tauref : as.tauref_in;
     sd.qextrefdst = as.qextrefdst;
     sd.qxvdst = as.qxvdst;
     sd.qsvdst = as.qsvdst;
@@ -1347,6 +1355,9 @@ mgcm_rt_handle *mgcm_rt_create(const mgcm_rt_config *cfg, const char *data_dir, 
                 for (int j = 0; j < AERO_NRATIO; ++j)
                     for (int i = 0; i < AERO_NBIN; ++i)
                         for (int l = 0; l < AERO_NI; ++l) mie.push_back(at.cld_i[m][j][i][l]);
+            // then the prescribed dust band properties (SegDev::dust_band order)
+            for (const double *p : {A.qextv, A.qscatv, A.gv}) mie.insert(mie.end(), p, p + AERO_NV);
+            for (const double *p : {A.qexti, A.qscati, A.gi}) mie.insert(mie.end(), p, p + AERO_NI);
             if (cudaMalloc(&h->d_mie, mie.size() * 8) ||
                 cudaMemcpy(h->d_mie, mie.data(), mie.size() * 8, cudaMemcpyHostToDevice))
                 return fail(MGCM_RT_ENOMEM);

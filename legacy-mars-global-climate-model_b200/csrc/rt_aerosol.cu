@@ -191,10 +191,19 @@ rt_aerosol(const AeroSeg a, const AeroConst K, const double *__restrict__ mie) {
          cc += (long long)gridDim.x * AERO_WARPS) {
         const size_t c = (size_t)cc;
         const double *pl = a.plev + c * lev;
-        double *tr = a.tauref + c * lev1, *qr = a.qextrefdst + c * lev1;
-        double *xv = a.qxvdst + c * AERO_NV * lev1, *sv = a.qsvdst + c * AERO_NV * lev1;
-        double *gv = a.gvdst + c * AERO_NV * lev1, *xi = a.qxidst + c * AERO_NI * lev1;
-        double *si = a.qsidst + c * AERO_NI * lev1, *gi = a.gidst + c * AERO_NI * lev1;
+        // dust arrays (absent for prescribed dust read as band constants)
+        double *tr = nullptr, *qr = nullptr, *xv = nullptr, *sv = nullptr, *gv = nullptr;
+        double *xi = nullptr, *si = nullptr, *gi = nullptr;
+        if (a.tauref) {
+            tr = a.tauref + c * lev1;
+            qr = a.qextrefdst + c * lev1;
+            xv = a.qxvdst + c * AERO_NV * lev1;
+            sv = a.qsvdst + c * AERO_NV * lev1;
+            gv = a.gvdst + c * AERO_NV * lev1;
+            xi = a.qxidst + c * AERO_NI * lev1;
+            si = a.qsidst + c * AERO_NI * lev1;
+            gi = a.gidst + c * AERO_NI * lev1;
+        }
         double *tc = nullptr, *qc = nullptr, *cxv = nullptr, *csv = nullptr, *cgv = nullptr;
         double *cxi = nullptr, *csi = nullptr, *cgi = nullptr;
         if (a.cloudon) {
@@ -231,13 +240,16 @@ rt_aerosol(const AeroSeg a, const AeroConst K, const double *__restrict__ mie) {
         __syncwarp();
         // every other level: prescribed dust or the routines' defaults (levels
         // 1-3 and L_LEVELS+1 always), a lane per level
-        const double *tin = a.tauref_in + c * lev1;
+        const double *tin = a.tauref_in ? a.tauref_in + c * lev1 : nullptr;
         for (int k = lane + 1; k <= lev1; k += 32) {
             const int l = (k >= 4 && k <= lev) ? (k - 2) / 2 : 0;
             const bool d_act = l && ((dmask[(l - 1) >> 5] >> ((l - 1) & 31)) & 1u);
             const bool c_act = l && ((cmask[(l - 1) >> 5] >> ((l - 1) & 31)) & 1u);
-            if (!a.active_dust) prescribed_level(K, lev1, k, tin, tr, qr, xv, sv, gv, xi, si, gi);
-            else if (!d_act) default_level(lev1, k, tr, qr, xv, sv, gv, xi, si, gi);
+            if (!a.active_dust) {
+                if (tr) prescribed_level(K, lev1, k, tin, tr, qr, xv, sv, gv, xi, si, gi);
+            } else if (!d_act) {
+                default_level(lev1, k, tr, qr, xv, sv, gv, xi, si, gi);
+            }
             if (a.cloudon && !c_act) default_level(lev1, k, tc, qc, cxv, csv, cgv, cxi, csi, cgi);
         }
         // the layers with aerosol, one at a time across the warp

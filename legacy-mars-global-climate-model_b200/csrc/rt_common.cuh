@@ -59,6 +59,12 @@ struct SegDev {
     const double *sigma, *sol;
     const double *plev, *tlev, *pmid, *tmid, *qh2o;
     const double *tauref, *qextrefdst, *taurefcld, *qextrefcld;
+    // Prescribed dust (INI_OPTDST): when set, these 36 band properties --
+    // QEXTV[7], QSCATV[7], GV[7], QEXTI[5], QSCATI[5], GI[5] -- stand for the
+    // per-level dust arrays (the same values at every level), QEXTREFDST is
+    // QEXTV(L_NREFV) and TAUREF(L_LEVELS+1) is 0 (code/ini_optdst.f:29-51,
+    // code/comp3.f:618); the qx/qs/g dust pointers are then unused.
+    const double *dust_band;
     const double *qxvdst, *qsvdst, *gvdst, *qxidst, *qsidst, *gidst;
     const double *qxvcld, *qsvcld, *gvcld, *qxicld, *qsicld, *gicld;
     const double *acosz, *als, *albi, *pcol;

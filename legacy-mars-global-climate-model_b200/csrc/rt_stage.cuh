@@ -16,8 +16,9 @@ __device__ inline void stage_level(const SegDev &sg, int c, const RtConst &K, Co
     const double *tmid = sg.tmid + (size_t)c * LEV;
     const double *qh2o = sg.qh2o + (size_t)c * LEV;
     const double *tauref = sg.tauref + (size_t)c * LEV1;
-    const double *qxref = sg.qextrefdst + (size_t)c * LEV1;
-    const double *qxv = sg.qxvdst + (size_t)c * D_NV * LEV1;
+    const double *db = sg.dust_band;   // prescribed dust: band constants
+    const double *qxref = db ? nullptr : sg.qextrefdst + (size_t)c * LEV1;
+    const double *qxv = db ? nullptr : sg.qxvdst + (size_t)c * D_NV * LEV1;
     const bool cld = sg.taurefcld != nullptr;
     const double *taucld = cld ? sg.taurefcld + (size_t)c * LEV1 : nullptr;
     const double *qxcld = cld ? sg.qextrefcld + (size_t)c * LEV1 : nullptr;
@@ -38,11 +39,11 @@ __device__ inline void stage_level(const SegDev &sg, int c, const RtConst &K, Co
             const double dpr = plev[k - 1] - plev[k - 2];
             s.dpr[k] = dpr;
             s.u[k] = 3.51e22 * dpr;
-            s.tref_v[k] = tauref[k - 1] / qxv[(size_t)(NREFV_IDX)*LEV1 + k - 1];
-            s.tref_i[k] = tauref[k - 1] / qxref[k - 1];
+            s.tref_v[k] = tauref[k - 1] / (db ? db[NREFV_IDX] : qxv[(size_t)(NREFV_IDX)*LEV1 + k - 1]);
+            s.tref_i[k] = tauref[k - 1] / (db ? db[NREFV_IDX] : qxref[k - 1]);
             s.tref_c[k] = cld ? taucld[k - 1] / qxcld[k - 1] : 0.0 / 1.0;
         } else {
-            s.tref_i[k] = tauref[k - 1];
+            s.tref_i[k] = db ? 0.0 : tauref[k - 1];
             s.tref_c[k] = cld ? taucld[k - 1] : 0.0;
         }
     }
@@ -63,21 +64,24 @@ __device__ inline void stage_band(const SegDev &sg, int c, const RtConst &K,
     {
         if (it < nitem_v) {
             const int l = it / D_NV, nw = it % D_NV + 1;
-            const double *qx = sg.qxvdst + ((size_t)c * D_NV + nw - 1) * LEV1;
-            const double *qs = sg.qsvdst + ((size_t)c * D_NV + nw - 1) * LEV1;
-            const double *gv = sg.gvdst + ((size_t)c * D_NV + nw - 1) * LEV1;
+            // dust properties of level k at qx[(k - 1) * ks] (ks = 0: band constants)
+            const double *db = sg.dust_band;
+            const int ks = db ? 0 : 1;
+            const double *qx = db ? db + nw - 1 : sg.qxvdst + ((size_t)c * D_NV + nw - 1) * LEV1;
+            const double *qs = db ? db + D_NV + nw - 1 : sg.qsvdst + ((size_t)c * D_NV + nw - 1) * LEV1;
+            const double *gv = db ? db + 2 * D_NV + nw - 1 : sg.gvdst + ((size_t)c * D_NV + nw - 1) * LEV1;
             const double *qxc = cld ? sg.qxvcld + ((size_t)c * D_NV + nw - 1) * LEV1 : nullptr;
             const double *qsc = cld ? sg.qsvcld + ((size_t)c * D_NV + nw - 1) * LEV1 : nullptr;
             const double *gc = cld ? sg.gvcld + ((size_t)c * D_NV + nw - 1) * LEV1 : nullptr;
             const double tr0 = K.tauray[nw - 1];
             auto lvl = [&](int k, double &tr, double &tl, double &tc, double &g1, double &g2) {
                 tr = tr0 * s.dpr[k];
-                const double taeros = s.tref_v[k] * qx[k - 1];
+                const double taeros = s.tref_v[k] * qx[(k - 1) * ks];
                 const double tcloud = s.tref_c[k] * (cld ? qxc[k - 1] : 0.0);
                 s.trayaer[k * D_NV + nw - 1] = tr + taeros + tcloud;
-                tl = s.tref_v[k] * qs[k - 1];
+                tl = s.tref_v[k] * qs[(k - 1) * ks];
                 tc = s.tref_c[k] * (cld ? qsc[k - 1] : 0.0);
-                g1 = gv[k - 1];
+                g1 = gv[(k - 1) * ks];
                 g2 = cld ? gc[k - 1] : 0.0;
             };
             double tra, tla, tca, ga, gca;
@@ -100,14 +104,18 @@ __device__ inline void stage_band(const SegDev &sg, int c, const RtConst &K,
         } else if (it < nitem_v + nitem_i) {
             const int j = it - nitem_v;
             const int l = j / D_NI, nw = j % D_NI + 1;
-            const double *qx = sg.qxidst + ((size_t)c * D_NI + nw - 1) * LEV1;
-            const double *qs = sg.qsidst + ((size_t)c * D_NI + nw - 1) * LEV1;
-            const double *gi = sg.gidst + ((size_t)c * D_NI + nw - 1) * LEV1;
+            const double *db = sg.dust_band;
+            const int ks = db ? 0 : 1;
+            const double *qx = db ? db + 3 * D_NV + nw - 1 : sg.qxidst + ((size_t)c * D_NI + nw - 1) * LEV1;
+            const double *qs = db ? db + 3 * D_NV + D_NI + nw - 1
+                                  : sg.qsidst + ((size_t)c * D_NI + nw - 1) * LEV1;
+            const double *gi = db ? db + 3 * D_NV + 2 * D_NI + nw - 1
+                                  : sg.gidst + ((size_t)c * D_NI + nw - 1) * LEV1;
             const double *qxc = cld ? sg.qxicld + ((size_t)c * D_NI + nw - 1) * LEV1 : nullptr;
             const double *qsc = cld ? sg.qsicld + ((size_t)c * D_NI + nw - 1) * LEV1 : nullptr;
             const double *gc = cld ? sg.gicld + ((size_t)c * D_NI + nw - 1) * LEV1 : nullptr;
             auto ext = [&](int k) {   // TAEROS, TCLOUD at level k <= LEV
-                s.taer_i[k * D_NI + nw - 1] = s.tref_i[k] * qx[k - 1];
+                s.taer_i[k * D_NI + nw - 1] = s.tref_i[k] * qx[(k - 1) * ks];
                 s.tcld_i[k * D_NI + nw - 1] = s.tref_c[k] * (cld ? qxc[k - 1] : 0.0);
             };
             if (l == 0) {
@@ -116,14 +124,14 @@ __device__ inline void stage_band(const SegDev &sg, int c, const RtConst &K,
                 const int k = 2 * l + 1;
                 ext(k);
                 if (k + 1 <= LEV) ext(k + 1);
-                const double tla = s.tref_i[k] * qs[k - 1], tlb = s.tref_i[k + 1] * qs[k];
+                const double tla = s.tref_i[k] * qs[(k - 1) * ks], tlb = s.tref_i[k + 1] * qs[k * ks];
                 const double tca = s.tref_c[k] * (cld ? qsc[k - 1] : 0.0);
                 const double tcb = s.tref_c[k + 1] * (cld ? qsc[k] : 0.0);
                 const double tauac = tla + tlb + tca + tcb;
                 s.wnum_i[l * D_NI + nw - 1] = tauac;
                 double cb = 0.0;
                 if (tauac > 0.0)
-                    cb = (gi[k - 1] * tla + gi[k] * tlb + (cld ? gc[k - 1] : 0.0) * tca +
+                    cb = (gi[(k - 1) * ks] * tla + gi[k * ks] * tlb + (cld ? gc[k - 1] : 0.0) * tca +
                           (cld ? gc[k] : 0.0) * tcb) /
                          (tla + tlb + tca + tcb);
                 s.cosb_i[l * D_NI + nw - 1] = cb;
