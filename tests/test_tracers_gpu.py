@@ -82,3 +82,21 @@ def test_tracers_argument_errors(data_dir):
         assert e.value.code == -4
     finally:
         rt.close()
+
+
+@pytest.mark.parametrize("active_dust,cloudon", [(0, 1), (1, 1), (0, 0)])
+def test_tracers_equal_arrays_path_bitwise(data_dir, aero, active_dust, cloudon):
+    """The tracer call (device aerosol optics; prescribed dust read as band
+    constants; ice properties read only where TAUREFCLD != 0) gives the same
+    bits as the drop-in call on the oracle's full per-level aerosol arrays."""
+    tb = synth.make_tracer_batch(300, L=24, seed=470 + 2 * active_dust + cloudon,
+                                 active_dust=bool(active_dust), cloudon=bool(cloudon))
+    full = oracle.aerosols(aero, tb)
+    rt = abi.Radiation(data_dir, max_layers=24, precision=abi.FP64, validate=True)
+    try:
+        a = to_numpy(rt.run_tracers(tb))
+        b = to_numpy(rt.run(full))
+        for k in b:
+            np.testing.assert_array_equal(a[k], b[k], err_msg=k)
+    finally:
+        rt.close()
