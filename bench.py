@@ -96,6 +96,24 @@ def peaks():
         return 6650.0, "fallback"
 
 
+def fp64_pipe(L: int, ncol: float, seconds: float):
+    """Second ceiling of the roofline: the reference's floating-point
+    operations per column (bench/algorithmic_counts.json, counted on the CPU
+    oracle; exp/div/sqrt one each) over the call time, against the measured
+    FP64 FMA-chain peak (profiles/fp_pipe_peaks.json).  None without them."""
+    try:
+        counts = json.loads((ROOT / "bench" / "algorithmic_counts.json").read_text())
+        per = next(w["per_column"] for w in counts["workloads"].values() if int(w["layers"]) == L)
+        peak = float(json.loads((ROOT / "profiles" / "fp_pipe_peaks.json").read_text())["fp64_fma_tflops"])
+    except Exception:
+        return None
+    ach = per["flops"] * ncol / seconds / 1e12
+    return {"achieved": ach, "peak": peak, "unit": "TFLOP/s", "frac": ach / peak,
+            "flops_per_column": per["flops"], "div_per_column": per["div"], "exp_per_column": per["exp"],
+            "gathers_per_column": per["gather"],
+            "counts": "bench/algorithmic_counts.json", "peak_source": "profiles/fp_pipe_peaks.json"}
+
+
 class Clocks:
     """nvidia-smi sampling during the timed region."""
 
@@ -630,7 +648,8 @@ def main():
             "roofline": {"bound": "hbm", "achieved": ach, "peak": pk, "unit": "GB/s",
                          "frac": ach / pk, "traffic": traffic_per_step(hp, ncol, L),
                          "kernel": "radiation pipeline (stage, screen, 2 solves, reduce) per call",
-                         "bytes_per_column": bpc, "kernel_ms": kms, "peak_kind": pk_kind},
+                         "bytes_per_column": bpc, "kernel_ms": kms, "peak_kind": pk_kind,
+                         "fp64_pipe": fp64_pipe(L, ncol, kms / 1e3)},
             "systems_per_step": st["systems"],
             "clocks": clk_summary,
         }

@@ -29,6 +29,12 @@
 
 #define R4(x) ((double)(float)(x))
 
+/* Table-gather hook for the operation-count build (oracle/orc_count.cpp);
+ * nothing in the normal builds. */
+#ifndef ORC_GATHERS
+#define ORC_GATHERS(n) ((void)0)
+#endif
+
 /* Per-column exponentials use the shared deterministic exp so the oracle and
  * the FP64 device path agree bit-for-bit (see include/mgcm_rt_math.h for why
  * the reference IR solver needs this).  Built with -DORC_LIBM_EXP the oracle
@@ -425,6 +431,7 @@ static void optcv(const orc_tables *t, const colview *c, work_t *w) {
                 /* CO2V(mt,mp,nh,nw,ng) with Fortran's linear addressing, so
                  * nh+1 = 11 reads the next band's first water slot exactly as
                  * the reference does (it is then multiplied by WRATIO = 0). */
+                ORC_GATHERS(8); /* CO2V corners read below */
 #define CV(a, b, h) t->co2v[(a - 1) + ORC_NTREF * ((b - 1) + ORC_PINT * ((h - 1) + ORC_REFH2O * ((nw - 1) + NB * (ng - 1))))]
                 double k1 = CV(mt, mp, nh) + wr * (CV(mt, mp, nh + 1) - CV(mt, mp, nh));
                 double k2 = CV(mt, mp + 1, nh) + wr * (CV(mt, mp + 1, nh + 1) - CV(mt, mp + 1, nh));
@@ -533,6 +540,7 @@ static void optci(const orc_tables *t, const colview *c, work_t *w) {
         const double *lk = &w->lk[k * 4];
         for (int nw = 1; nw <= NB; nw++) {
             for (int ng = 1; ng <= NG - 1; ng++) {
+                ORC_GATHERS(8); /* CO2I corners read below */
 #define CI(a, b, h) t->co2i[(a - 1) + ORC_NTREF * ((b - 1) + ORC_PINT * ((h - 1) + ORC_REFH2O * ((nw - 1) + NB * (ng - 1))))]
                 double k1 = CI(mt, mp, nh) + wr * (CI(mt, mp, nh + 1) - CI(mt, mp, nh));
                 double k2 = CI(mt, mp + 1, nh) + wr * (CI(mt, mp + 1, nh + 1) - CI(mt, mp + 1, nh));
@@ -1220,7 +1228,8 @@ int orc_aero_load(orc_aero *a, const char *dir) {
     }
     const size_t ncv = (size_t)ORC_NRATIO * ORC_NBIN * 3 * ORC_NSPECTV, nci = (size_t)ORC_NRATIO * ORC_NBIN * 3 * ORC_NSPECTI;
     const size_t ndv = (size_t)ORC_NBIN * 3 * ORC_NSPECTV, ndi = (size_t)ORC_NBIN * 3 * ORC_NSPECTI;
-    double *cv = malloc(ncv * 8), *ci = malloc(nci * 8), *dv = malloc(ndv * 8), *di = malloc(ndi * 8);
+    double *cv = (double *)malloc(ncv * sizeof(double)), *ci = (double *)malloc(nci * sizeof(double));
+    double *dv = (double *)malloc(ndv * sizeof(double)), *di = (double *)malloc(ndi * sizeof(double));
     char path[4096];
     int rc = 0;
     snprintf(path, sizeof path, "%s/waterCoated_vis_JD_12bands.dat", dir);

@@ -16,7 +16,8 @@ HERE = pathlib.Path(__file__).resolve().parent
 LIB = HERE / "_build" / "liboracle.so"
 # variant "libm": column exponentials from the host libm instead of the shared
 # deterministic exp (measures the reference algorithm's libm sensitivity)
-LIBS = {"rt": LIB, "libm": HERE / "_build" / "liboracle_libm.so"}
+LIBS = {"rt": LIB, "libm": HERE / "_build" / "liboracle_libm.so",
+        "count": HERE / "_build" / "liboracle_count.so"}
 
 NTAB_V = 7 * 51 * 10 * 7 * 17
 NTAB_I = 7 * 51 * 10 * 5 * 17
@@ -293,7 +294,7 @@ def jsrchgt(sx, target: float) -> int:
     return int(_prep_lib().orc_jsrchgt(len(a), _p(a), target))
 
 
-def prep(st: dict) -> dict:
+def prep(st: dict, variant: str = "rt") -> dict:
     """State batch (synth.make_state_batch) -> the tracer batch COMP3 would
     hand to the aerosol optics: PLEV/TLEV/PMID/TMID/QH2O, and TAUREF for
     prescribed dust, filled as the reference fills them."""
@@ -326,9 +327,25 @@ def prep(st: dict) -> dict:
     s.conr = inp("conr") if prescribed else None
     for k, v in out.items():
         setattr(s, k, v.ctypes.data if v is not None else None)
-    _prep_lib().orc_prep(C.byref(s))
+    _prep_lib(variant).orc_prep(C.byref(s))
     tb = {k: st[k] for k in ("ncol", "L", "ptrop", "sigma", "sol", "pcol", "acosz", "als", "albi",
                              "detau", "cumtauv", "dust_mass", "dust_number", "ice_mass", "ice_core_mass",
                              "ice_number", "active_dust", "cloudon")}
     tb.update(out)
     return tb
+
+
+# ---- operation counts (orc_count.cpp: the oracle with a counting number type)
+COUNT_KINDS = ("add", "mul", "div", "sqrt", "exp", "log", "pow", "erf", "gather")
+
+
+def op_counts(fn) -> dict:
+    """Run fn() -- a call into the "count" variant of the oracle on one
+    thread -- and return the floating-point operations it performed, by
+    kind (COUNT_KINDS)."""
+    L = lib("count")
+    out = (C.c_ulonglong * len(COUNT_KINDS))()
+    L.orc_count_reset()
+    fn()
+    L.orc_count_read(out)
+    return dict(zip(COUNT_KINDS, (int(v) for v in out)))

@@ -223,3 +223,29 @@ def test_oracle_reproduces_golden_vectors(otables, name):
     out = oracle.run_batch(otables, b)
     for k, v in out.items():
         np.testing.assert_allclose(np.asarray(v), g[k], rtol=1e-13, atol=1e-300, err_msg=k)
+
+
+def test_operation_count_build_reproduces_the_oracle(data_dir, otables):
+    """oracle/orc_count.cpp (the oracle with a counting number type) computes
+    the same bits as the oracle and counts the operations
+    bench/algorithmic_counts.json is built from."""
+    import json
+    import pathlib
+    tc = oracle.Tables(data_dir, variant="count")
+    b = synth.make_batch(24, L=24, seed=1000, cloud=True)
+    ref = oracle.run_batch(otables, b, 1)
+    got = {}
+    cnt = oracle.op_counts(lambda: got.update(oracle.run_batch(tc, b, 1)))
+    for k in ref:
+        np.testing.assert_array_equal(got[k], ref[k], err_msg=k)
+    # IR: 5 bands x 16 Gauss points x 50 levels x 8 corners per column;
+    # visible: 7 x 16 x 50 x 8 per day column
+    day = int(np.sum(np.asarray(b["acosz"]) >= 1.0e-5))
+    assert cnt["gather"] == 24 * 5 * 16 * 50 * 8 + day * 7 * 16 * 50 * 8
+    assert cnt["div"] > 0 and cnt["exp"] > 0 and cnt["sqrt"] > 0 and cnt["erf"] == 0
+    frozen = json.loads((pathlib.Path(__file__).resolve().parents[1] / "bench" /
+                         "algorithmic_counts.json").read_text())
+    c1 = frozen["workloads"]["c1"]["per_column"]
+    # the frozen per-column means are of the same order as this small sample's
+    flops = sum(cnt[k] for k in ("add", "mul", "div", "sqrt", "exp", "log", "pow", "erf")) / 24
+    assert 0.5 < flops / c1["flops"] < 2.0
