@@ -111,6 +111,8 @@ def fp64_pipe(L: int, ncol: float, seconds: float):
     return {"achieved": ach, "peak": peak, "unit": "TFLOP/s", "frac": ach / peak,
             "flops_per_column": per["flops"], "div_per_column": per["div"], "exp_per_column": per["exp"],
             "gathers_per_column": per["gather"],
+            # the third ceiling: k-table gathers (8-byte reads served by L1/L2)
+            "gather_gbs": per["gather"] * 8 * ncol / seconds / 1e9,
             "counts": "bench/algorithmic_counts.json", "peak_source": "profiles/fp_pipe_peaks.json"}
 
 
@@ -199,8 +201,26 @@ def cpu_baseline(batch, data_dir, budget_s=10.0, tracers=None):
     run(sub(n))
     dt = time.perf_counter() - t0
     what = "aerosol optics + radiation" if a is not None else "radiation"
+    # one core: the reference itself runs its column loop on one core
+    run1 = (lambda b: _oracle_call(t, a, b, 1)) if a is not None else (lambda b: oracle.run_batch(t, b, 1))
+    n1 = int(min(src["ncol"], max(16, 0.3 * budget_s / max(per * cores, 1e-9))))
+    t0 = time.perf_counter()
+    run1(sub(n1))
+    dt1 = time.perf_counter() - t0
     return {"value": n / dt, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"first {n} columns of the workload ({what}), {dt:.1f} s on {cores} threads"}
+            "sample": f"first {n} columns of the workload ({what}), {dt:.1f} s on {cores} threads",
+            "one_core": {"value": n1 / dt1, "unit": UNIT, "sample": f"first {n1} columns, {dt1:.1f} s on 1 thread"},
+            "cpu_model": cpu_model()}
+
+
+def cpu_model() -> str:
+    try:
+        for line in pathlib.Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
 
 
 def run_reference(args, wl):
