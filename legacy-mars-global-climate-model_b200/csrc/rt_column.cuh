@@ -17,14 +17,24 @@ __device__ __forceinline__ int find_seg(const SegTable *__restrict__ st, int g) 
     return s;
 }
 
+// What every system's k-table gather needs of level k (tpindex and U), in
+// one 64-byte record so a thread fetches it with four 16-byte loads: the
+// bilinear weights LCOEF(1..4), WRATIO, U = Cmk*DPR, the element offset of
+// the (MT, MP, NH2O) corner within a band's table and the step to the
+// NH2O+1 row (0 where NH2O = 10, whose WRATIO is 0).
+struct alignas(16) KLevel {
+    double lk[4];
+    double wr, u;
+    int kofs, kdh;
+    int pad[2];
+};
+static_assert(sizeof(KLevel) == 64, "KLevel is one 64-byte record");
+
 // Shared-memory layout of one column; sized by the launch's largest NL.
 struct ColSmem {
-    // per level (1-based k = 1..LEV+1): the k-table gather of the level's
-    // bins (tpindex MT, MP, NH2O) as one element offset of the (MT, MP, NH2O)
-    // corner within a band's table, and the step to the NH2O+1 row (0 where
-    // NH2O = 10, whose WRATIO is 0)
-    int *kofs, *kdh;
-    double *wr, *lk, *u, *dpr;
+    // per level (1-based k = 1..LEV+1)
+    KLevel *klev;
+    double *dpr;
     double *tref_v, *tref_i, *tref_c;   // TAUREF/QEXTREF (vis, IR), TAUREFCLD/QEXTREFCLD
     // per level and band
     double *trayaer;                    // [k][7] visible TRAY+TAEROS+TCLOUD
@@ -55,8 +65,8 @@ __host__ __device__ inline size_t red_bytes(int nl) { return 2 * (size_t)NSYS * 
 __host__ __device__ inline size_t col_smem_bytes(int nl, bool red_in_smem = true) {
     const size_t lev1 = 2 * nl + 3;   // 1-based k up to LEV+1 = 2L+4 = 2NL+2
     size_t b = 0;
-    b += 2 * (lev1 + 1) * sizeof(int);
-    b += (lev1 + 1) * (1 + 4 + 1 + 1 + 3) * sizeof(double);
+    b += (lev1 + 1) * sizeof(KLevel);
+    b += (lev1 + 1) * (1 + 3) * sizeof(double);
     b += (lev1 + 1) * (D_NV + 2 * D_NI) * sizeof(double);
     b += (nl + 1) * (2 * D_NV + 4 * D_NI) * sizeof(double);
     b += 2 * D_NI * sizeof(double);
@@ -71,11 +81,9 @@ __device__ inline ColSmem carve_smem(unsigned char *base, int nl, double *red_gl
                                      bool with_red = true) {
     ColSmem s;
     const int lev1 = 2 * nl + 3;
-    double *d = reinterpret_cast<double *>(base);
+    s.klev = reinterpret_cast<KLevel *>(base);   // base is 16-byte aligned
+    double *d = reinterpret_cast<double *>(base + (size_t)(lev1 + 1) * sizeof(KLevel));
     auto take = [&](size_t n) { double *p = d; d += n; return p; };
-    s.wr = take(lev1 + 1);
-    s.lk = take(4 * (lev1 + 1));
-    s.u = take(lev1 + 1);
     s.dpr = take(lev1 + 1);
     s.tref_v = take(lev1 + 1);
     s.tref_i = take(lev1 + 1);
@@ -107,9 +115,7 @@ __device__ inline ColSmem carve_smem(unsigned char *base, int nl, double *red_gl
     s.fmnet_i = take(nl + 1);
     s.misc = take(4);
     int *ip = reinterpret_cast<int *>(d);
-    s.kofs = ip;
-    s.kdh = ip + (lev1 + 1);
-    s.skip = reinterpret_cast<unsigned char *>(ip + 2 * (lev1 + 1));
+    s.skip = reinterpret_cast<unsigned char *>(ip);
     s.meta = reinterpret_cast<int *>(((reinterpret_cast<uintptr_t>(s.skip + NSYS) + 15) / 16) * 16);
     s.day = 0;
     return s;

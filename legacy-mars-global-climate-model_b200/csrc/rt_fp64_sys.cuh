@@ -117,34 +117,51 @@ constexpr int KT_DP = D_NH * D_NGK, KT_DT = D_NP * D_NH * D_NGK;
 // 8-corner gather and interpolation (optcv.f90:279-301): returns TAUGAS.
 // tb points at the band's table plus the Gauss point; the level's corner
 // offset and NH2O step come staged (ColSmem::kofs, kdh).
+// The level's record, four 16-byte loads.
+struct KLv {
+    double2 lk01, lk23, wu;
+    int2 kd;
+};
+__device__ __forceinline__ KLv klev_load(const ColSmem &s, int k) {
+    const double2 *q = reinterpret_cast<const double2 *>(s.klev + k);
+    KLv r;
+    r.lk01 = q[0];
+    r.lk23 = q[1];
+    r.wu = q[2];
+    r.kd = *reinterpret_cast<const int2 *>(q + 3);
+    return r;
+}
+
 __device__ __forceinline__ double taugas_at(const ColSmem &s, int k, const double *__restrict__ tb) {
-    const double *p = tb + s.kofs[k];
-    const int dh = s.kdh[k];
-    const double wr = s.wr[k];
+    const KLv kl = klev_load(s, k);
+    const double *p = tb + kl.kd.x;
+    const int dh = kl.kd.y;
+    const double wr = kl.wu.x;
     auto corner = [&](int off) {
         const double c0 = __ldg(p + off), c1 = __ldg(p + off + dh);
         return c0 + wr * (c1 - c0);
     };
     const double k1 = corner(0), k2 = corner(KT_DP);
     const double k3 = corner(KT_DT + KT_DP), k4 = corner(KT_DT);
-    const double ans = s.lk[4 * k] * k1 + s.lk[4 * k + 1] * k2 + s.lk[4 * k + 2] * k3 + s.lk[4 * k + 3] * k4;
-    return s.u[k] * ans;
+    const double ans = kl.lk01.x * k1 + kl.lk01.y * k2 + kl.lk23.x * k3 + kl.lk23.y * k4;
+    return kl.wu.y * ans;
 }
 
 
 // TAUGAS at level k from the FP32 table of Cmk*k (mixed precision).
 __device__ __forceinline__ float taugas_f(const ColSmem &s, int k, const float *__restrict__ tb) {
-    const float *p = tb + s.kofs[k];
-    const int dh = s.kdh[k];
-    const float wr = (float)s.wr[k];
+    const KLv kl = klev_load(s, k);
+    const float *p = tb + kl.kd.x;
+    const int dh = kl.kd.y;
+    const float wr = (float)kl.wu.x;
     auto corner = [&](int off) {
         const float c0 = __ldg(p + off), c1 = __ldg(p + off + dh);
         return c0 + wr * (c1 - c0);
     };
     const float k1 = corner(0), k2 = corner(KT_DP);
     const float k3 = corner(KT_DT + KT_DP), k4 = corner(KT_DT);
-    const float ans = (float)s.lk[4 * k] * k1 + (float)s.lk[4 * k + 1] * k2 +
-                      (float)s.lk[4 * k + 2] * k3 + (float)s.lk[4 * k + 3] * k4;
+    const float ans = (float)kl.lk01.x * k1 + (float)kl.lk01.y * k2 +
+                      (float)kl.lk23.x * k3 + (float)kl.lk23.y * k4;
     return (float)s.dpr[k] * ans;
 }
 

@@ -29,16 +29,17 @@ __device__ inline void stage_level(const SegDev &sg, int c, const RtConst &K, Co
             double wr, lk[4];
             tpindex_dev(K, pmid[k - 1], tmid[k - 1], qh2o[k - 1], mt, mp, nh, wr, lk);
             const int nh1 = nh < D_NH ? nh + 1 : D_NH;   // WRATIO = 0 when NH2O = 10
-            s.kofs[k] = (((mt - 1) * D_NP + (mp - 1)) * D_NH + (nh - 1)) * D_NGK;
-            s.kdh[k] = (nh1 - nh) * D_NGK;
-            s.wr[k] = wr;
-            s.lk[4 * k + 0] = lk[0];
-            s.lk[4 * k + 1] = lk[1];
-            s.lk[4 * k + 2] = lk[2];
-            s.lk[4 * k + 3] = lk[3];
+            KLevel &kl = s.klev[k];
+            kl.kofs = (((mt - 1) * D_NP + (mp - 1)) * D_NH + (nh - 1)) * D_NGK;
+            kl.kdh = (nh1 - nh) * D_NGK;
+            kl.wr = wr;
+            kl.lk[0] = lk[0];
+            kl.lk[1] = lk[1];
+            kl.lk[2] = lk[2];
+            kl.lk[3] = lk[3];
             const double dpr = plev[k - 1] - plev[k - 2];
             s.dpr[k] = dpr;
-            s.u[k] = 3.51e22 * dpr;
+            kl.u = 3.51e22 * dpr;
             s.tref_v[k] = tauref[k - 1] / (db ? db[NREFV_IDX] : qxv[(size_t)(NREFV_IDX)*LEV1 + k - 1]);
             s.tref_i[k] = tauref[k - 1] / (db ? db[NREFV_IDX] : qxref[k - 1]);
             s.tref_c[k] = cld ? taucld[k - 1] / qxcld[k - 1] : 0.0 / 1.0;
