@@ -273,7 +273,7 @@ template __global__ void rt_quad_solve<false, 13>(QUAD_ARGS);
 // its outputs over the rows in the reference order (rows are in ascending
 // (band, Gauss) order, each scaled by the multipliers of family_multipliers).
 constexpr int RED_WARPS = 4;
-constexpr int RED_STAGES = 4;
+constexpr int RED_STAGES = 2;
 constexpr int RED_LPL = (D_MAXNL + 1 + 31) / 32;   // levels per lane
 
 __host__ __device__ inline size_t red_warp_bytes(int max_nl, int rb) {
