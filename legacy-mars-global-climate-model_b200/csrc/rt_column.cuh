@@ -41,6 +41,7 @@ struct ColSmem {
     double *taer_i, *tcld_i;            // [k][5] IR TAEROS, TCLOUD
     // per layer and band
     double *cosb_v, *wnum_v;            // [l][7]
+    double *cbs_v;                      // [l][7] COSBV/(1+COSBV), the delta-Eddington COSBAR
     double *cosb_i, *wnum_i;            // [l][5]
     double *b0_i, *pdif_i;              // [l][5] Planck B0 and B1*DTAU numerator
     double *bsurf_i, *pltop_i;          // [5]
@@ -68,7 +69,7 @@ __host__ __device__ inline size_t col_smem_bytes(int nl, bool red_in_smem = true
     b += (lev1 + 1) * sizeof(KLevel);
     b += (lev1 + 1) * (1 + 3) * sizeof(double);
     b += (lev1 + 1) * (D_NV + 2 * D_NI) * sizeof(double);
-    b += (nl + 1) * (2 * D_NV + 4 * D_NI) * sizeof(double);
+    b += (nl + 1) * (3 * D_NV + 4 * D_NI) * sizeof(double);
     b += 2 * D_NI * sizeof(double);
     if (red_in_smem) b += red_bytes(nl);
     b += 3 * NSYS * sizeof(double);
@@ -93,6 +94,7 @@ __device__ inline ColSmem carve_smem(unsigned char *base, int nl, double *red_gl
     s.tcld_i = take((lev1 + 1) * D_NI);
     s.cosb_v = take((nl + 1) * D_NV);
     s.wnum_v = take((nl + 1) * D_NV);
+    s.cbs_v = take((nl + 1) * D_NV);
     s.cosb_i = take((nl + 1) * D_NI);
     s.wnum_i = take((nl + 1) * D_NI);
     s.b0_i = take((nl + 1) * D_NI);

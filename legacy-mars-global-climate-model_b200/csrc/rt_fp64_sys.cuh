@@ -190,7 +190,8 @@ __device__ void solve_vis(const SegDev &sg, int c, int nw, int ng, int sidx, Col
         return s.trayaer[k * D_NV + nw - 1];
     };
     // pass A: levels 2..LEV, TCIN prefix sums, delta-Eddington stream.
-    // a0 = W0, a1 = COSBAR, a2 = scaled DTAU, a3 = TAU (1..NL+1), a4 = TAUCUM(2l+1)
+    // a0 = W0, a2 = scaled DTAU, a3 = TAU (1..NL+1), a4 = TAUCUM(2l+1); the
+    // scaled COSBAR of a layer is staged in the column block (cbs_v)
     const double tc2 = 0.0 + dtauk(2);
     double tc = tc2, tau = 0.0, fprev = 0.0, tcE1 = 0.0, tcLev = 0.0;
     for (int l = 1; l <= NL; ++l) {
@@ -216,10 +217,7 @@ __device__ void solve_vis(const SegDev &sg, int c, int nw, int ng, int sidx, Col
         } else if (l < NL) {
             if (MODE != 1) w.a4[l] = tau + (tcA - tc) * fprev;
         }
-        if (MODE != 1) {
-            w.a0[l] = wb * (1.0 - cb * cb) / f;
-            w.a1[l] = cb / (1.0 + cb);
-        }
+        if (MODE != 1) w.a0[l] = wb * (1.0 - cb * cb) / f;
         const double dtl = dt * f;
         if (MODE != 1) {
             w.a2[l] = dtl;
@@ -255,7 +253,7 @@ __device__ void solve_vis(const SegDev &sg, int c, int nw, int ng, int sidx, Col
     const double s3 = (double)sqrtf(3.0f), s3h = (double)(sqrtf(3.0f) * 0.5f);
     const double bsurf = rsf * u0 * sg.sol[nw - 1] * mgcm_rt_exp(-dmin(detau / u0, MAXEXP));
     const double btop = 0.0;
-    // LAMDA, GAMA, AM overwrite W0, COSBAR, DTAU of the same layer; AP -> c5
+    // LAMDA, GAMA, AM overwrite W0, a1 (unused by pass A), DTAU of the same layer; AP -> c5
     double *LAM = w.a0, *GAM = w.a1, *AM = w.a2, *AP = w.c5;
     auto coef = [&](int l, double w0, double cb, double dtl, double et_top, double et_bot) {
         Lay y;
@@ -288,15 +286,16 @@ __device__ void solve_vis(const SegDev &sg, int c, int nw, int ng, int sidx, Col
     double et_bot = mgcm_rt_exp(-dmin(w.a3[NL + 1] / u0, MAXEXP));
     double et_top = mgcm_rt_exp(-dmin(w.a3[NL] / u0, MAXEXP));
     // layer NL-1's inputs are fetched one step ahead
-    double pw0 = w.a0[NL - 1], pcb = w.a1[NL - 1], pdt = w.a2[NL - 1], pa3 = w.a3[NL - 1];
-    Lay hi = coef(NL, w.a0[NL], w.a1[NL], w.a2[NL], et_top, et_bot);
+    const double *cbs = s.cbs_v + nw - 1;   // layer l at cbs[l * D_NV]
+    double pw0 = w.a0[NL - 1], pcb = cbs[(NL - 1) * D_NV], pdt = w.a2[NL - 1], pa3 = w.a3[NL - 1];
+    Lay hi = coef(NL, w.a0[NL], cbs[NL * D_NV], w.a2[NL], et_top, et_bot);
     double as, ds;
     bottom_row(hi, NL, bsurf, rsf, w, as, ds);
     for (int n = NL - 1; n >= 1; --n) {
         const double w0 = pw0, cb = pcb, dtl = pdt, a3n = pa3;
         if (n > 1) {
             pw0 = w.a0[n - 1];
-            pcb = w.a1[n - 1];
+            pcb = cbs[(n - 1) * D_NV];
             pdt = w.a2[n - 1];
             pa3 = w.a3[n - 1];
         }

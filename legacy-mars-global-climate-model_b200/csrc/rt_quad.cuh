@@ -70,7 +70,7 @@ __device__ __forceinline__ void quad_vis(const SegDev &sg, int c, int nw, int ng
             const double f = 1.0 - wb * (cb * cb);
             fv[j] = f;
             w0v[j] = wb * (1.0 - cb * cb) / f;
-            cbv[j] = cb / (1.0 + cb);
+            cbv[j] = s.cbs_v[l * D_NV + nw - 1];
             dtl[j] = dt * f;
         }
     }

@@ -93,13 +93,16 @@ __device__ inline void stage_band(const SegDev &sg, int c, const RtConst &K,
                 double trb, tlb, tcb, gb, gcb;
                 lvl(k, tra, tla, tca, ga, gca);
                 lvl(k + 1, trb, tlb, tcb, gb, gcb);
-                s.cosb_v[l * D_NV + nw - 1] = (ga * tla + gb * tlb + gca * tca + gcb * tcb) /
-                                              (tra + trb + tla + tlb + tca + tcb);
+                const double cb = (ga * tla + gb * tlb + gca * tca + gcb * tcb) / (tra + trb + tla + tlb + tca + tcb);
+                s.cosb_v[l * D_NV + nw - 1] = cb;
+                s.cbs_v[l * D_NV + nw - 1] = cb / (1.0 + cb);   // code/getdetau.f90:308-335
                 s.wnum_v[l * D_NV + nw - 1] = tla + tlb + tca + tcb + (tra + trb) * R4(0.9999);
             } else {
                 const int k = LEV;
                 lvl(k, tra, tla, tca, ga, gca);
-                s.cosb_v[l * D_NV + nw - 1] = (ga * tla + gca * tca) / (tra + tla + tca);
+                const double cb = (ga * tla + gca * tca) / (tra + tla + tca);
+                s.cosb_v[l * D_NV + nw - 1] = cb;
+                s.cbs_v[l * D_NV + nw - 1] = cb / (1.0 + cb);
                 s.wnum_v[l * D_NV + nw - 1] = tla + tca + tra * R4(0.9999);
             }
         } else if (it < nitem_v + nitem_i) {
