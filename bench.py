@@ -64,7 +64,8 @@ WORKLOADS = {
 
 def algorithmic_bytes_per_column(L: int, cloud: bool) -> int:
     """Bytes the C ABI moves per column (FP64): inputs, outputs, DETAU and
-    CUMTAUV in and out.  8*(171L+696) with cloud; minus 8*38*(2L+4) without."""
+    CUMTAUV in and out (both are in/out arrays of the ABI).  8*(171L+815) with
+    cloud; minus 8*38*(2L+4) without."""
     lev, lev1, nl = 2 * L + 3, 2 * L + 4, L + 1
     n_in = 5 * lev + 2 * lev1 + 36 * lev1 + 4
     if cloud:
