@@ -207,3 +207,20 @@ def test_prep_structure():
     hi = np.maximum(tb["tlev"][:, 3:lev - 3:2], tb["tlev"][:, 5:lev - 1:2])
     mid = tb["tlev"][:, 4:lev - 2:2]
     assert np.all(mid >= lo - 1e-12) and np.all(mid <= hi + 1e-12)
+
+
+@pytest.mark.parametrize("L", [1, 2, 99])
+def test_prep_layer_count_edges(L):
+    """FILLPT's interpolation loop is empty at L = 1 and one level long at
+    L = 2; L = 99 is the largest layer count the library accepts."""
+    st = synth.make_state_batch(8, L=L, seed=40 + L, active_dust=False, cloudon=False,
+                                active_water=True, vary_conr=True)
+    tb = oracle.prep(st)
+    for c in range(st["ncol"]):
+        ref = py_prep_column(st, c)
+        for k in ("plev", "pmid", "qh2o"):
+            np.testing.assert_array_equal(tb[k][c], ref[k], err_msg=k)
+        for k in ("tlev", "tmid"):
+            np.testing.assert_allclose(tb[k][c], ref[k], rtol=1e-13, atol=0, err_msg=k)
+        tol = 1e-13 * float(st["tautot"][c])
+        np.testing.assert_allclose(tb["tauref"][c], ref["tauref"], rtol=1e-12, atol=tol)

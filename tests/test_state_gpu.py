@@ -59,6 +59,24 @@ def test_state_prep_bit_exact_and_fp64_parity(data_dir, otables, aero, case, L):
         rt.close()
 
 
+@pytest.mark.parametrize("L", [1, 2, 99])
+def test_state_layer_count_edges(data_dir, otables, aero, L):
+    """The smallest layer counts (FILLPT's interpolation loop empty or one
+    level long) and the largest the library accepts."""
+    st = _state(65, L, 790 + L, CASES[0])
+    tb = oracle.prep(st)
+    ref = oracle.run_batch(otables, oracle.aerosols(aero, tb))
+    rt = abi.Radiation(data_dir, max_layers=99, precision=abi.FP64, validate=True)
+    try:
+        got = to_numpy(rt.run_state(st, return_levels=True))
+        for k in abi.PREP_FIELDS:
+            np.testing.assert_array_equal(got[k], tb[k], err_msg=k)
+        err = compare(tb, got, ref, 1e-12)
+        assert max(err.values()) <= 1e-12, err
+    finally:
+        rt.close()
+
+
 def test_state_equals_tracers_on_prepared_arrays(data_dir):
     """After the prep the device path is the tracer path: same bits."""
     st = _state(300, 24, 760, CASES[0])
