@@ -30,7 +30,7 @@
  *   DETAU, CUMTAUV                [ncol][17][7]    (Fortran A(nw,ng,col))
  *
  * Errors are negative return codes (never abort/exit; the reference STOPs,
- * code/gfluxi.f90:215).  A handle is thread-safe: calls on one handle are
+ * code/gfluxi.f90:65).  A handle is thread-safe: calls on one handle are
  * serialised by an internal lock and run on the handle's own CUDA stream.
  */
 #ifndef MGCM_RT_H
@@ -42,10 +42,10 @@
 extern "C" {
 #endif
 
-#define MGCM_RT_NSPECTV 7    /* L_NSPECTV, code/modules.f90:224 */
-#define MGCM_RT_NSPECTI 5    /* L_NSPECTI, code/modules.f90:223 */
-#define MGCM_RT_NGAUSS 17    /* L_NGAUSS,  code/modules.f90:225 */
-#define MGCM_RT_MAX_LAYERS 99 /* NLL <= NLP = 101, code/gfluxi.f90:193,215 */
+#define MGCM_RT_NSPECTV 7    /* L_NSPECTV, code/modules.f90:225 */
+#define MGCM_RT_NSPECTI 5    /* L_NSPECTI, code/modules.f90:224 */
+#define MGCM_RT_NGAUSS 17    /* L_NGAUSS,  code/modules.f90:226 */
+#define MGCM_RT_MAX_LAYERS 99 /* NLL <= NLP = 101, code/gfluxi.f90:43,65 */
 
 /* precision modes */
 #define MGCM_RT_FP64 0  /* plain FP64, operation order of the reference */
@@ -125,9 +125,9 @@ typedef struct {
     int status;             /* device status word (0 = clean) */
 } mgcm_rt_stats;
 
-/* Reads CO2H2O_{V,IR}_12_95_INTEL from data_dir (code/laginterp.f90:220-230),
+/* Reads CO2H2O_{V,IR}_12_95_INTEL from data_dir (code/laginterp.f90:59-69),
  * builds the k tables (code/setrad.f90, code/laginterp.f90), the Planck table
- * (code/setspi.f90:245-259) and the band constants (code/setspv.f90), and
+ * (code/setspi.f90:91-105) and the band constants (code/setspv.f90), and
  * uploads them.  Replaces RADSETUP (code/radsetup.f90:26-43).
  * Returns NULL and sets *status on failure. */
 mgcm_rt_handle *mgcm_rt_create(const mgcm_rt_config *cfg, const char *data_dir, int *status);
@@ -192,7 +192,7 @@ int mgcm_rt_run_tracers(mgcm_rt_handle *h, const mgcm_rt_batch_tracers *in, mgcm
  * level pressures PL (code/potemp1.f:95-106) and FILLPT's PLEV, TLEV, PMID,
  * TMID (code/fillpt.f90:30-72), QH2O (code/comp3.f:576-589) and, for
  * prescribed dust, TAUREF from the Conrath profile of DUSTPROFILE sampled by
- * FILLTAUCUM (code/dustprofile.f:88-172, code/filltaucum.f:39-55).  Then the
+ * FILLTAUCUM (code/dustprofile.f:32-114, code/filltaucum.f:39-55).  Then the
  * aerosol optics and the radiation run as in mgcm_rt_run_tracers.  The host
  * passes the model state itself: about 1.6 KB per column at L = 24 with
  * dust and ice tracers.  COLDAIR stays on the host (it changes the model

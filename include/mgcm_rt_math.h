@@ -3,7 +3,7 @@
  *
  * The reference two-stream IR solver is ill-conditioned in optically thin
  * layers: EP = EXP(LAMDA*DTAU) enters the tridiagonal rows through EP-EM
- * (code/gfluxi.f90:263-273, code/dsolver.f90:74-80), so a one-ulp change of
+ * (code/gfluxi.f90:113-123, code/dsolver.f90:74-80), so a one-ulp change of
  * EXP moves IR fluxes by up to ~1e-6 relative (visible: ~1e-13).  Results of
  * the reference therefore depend on the libm it links.  To make the FP64 path
  * reproducible to 1e-12 across host and device, both the CPU oracle and the
@@ -192,14 +192,14 @@ MGCM_RT_HD double mgcm_rt_ln(double x) {
 }
 
 /* x**y for x > 0 as exp(y ln x) (the aerosol optics' real powers,
- * code/opt_dst.f:110, code/opt_cld.f:129).  Relative error about
+ * code/opt_dst.f:98,108, code/opt_cld.f:99,127,137).  Relative error about
  * (1 + |y ln x|) ulp. */
 MGCM_RT_HD double mgcm_rt_pow(double x, double y) {
     return mgcm_rt_exp(MGCM_RT_MUL(y, mgcm_rt_ln(x)));
 }
 
 /* Error function (the DERF of the aerosol size-bin weights,
- * code/opt_dst.f:120-121).  |x| < 1.5: Maclaurin series
+ * code/opt_dst.f:116-117).  |x| < 1.5: Maclaurin series
  *   erf x = 2/sqrt(pi) sum_n (-1)^n x^(2n+1) / (n! (2n+1)),
  * each term the previous one times -x^2 times the reciprocals 1/n and
  * 1/(2n+1) (correctly rounded: constants once the device unrolls the loop,

@@ -1315,7 +1315,7 @@ mgcm_rt_handle *mgcm_rt_create(const mgcm_rt_config *cfg, const char *data_dir, 
     std::vector<double> kv, ki;
     gauss_fastest(h->host, kv, ki);
     // FP32 tables hold Cmk*k (optical depth per mbar): k itself reaches 1e-49,
-    // below the FP32 range (code/optcv.f90:241-242, U = Cmk*DPR)
+    // below the FP32 range (code/optcv.f90:104-105,164, U = Cmk*DPR)
     std::vector<float> kvf(kv.size());
     for (size_t q = 0; q < kv.size(); ++q) kvf[q] = (float)(3.51e22 * kv[q]);
     if (cudaMalloc(&h->d_kv, kv.size() * 8) || cudaMalloc(&h->d_ki, ki.size() * 8) ||

@@ -123,7 +123,7 @@ __device__ inline ColSmem carve_smem(unsigned char *base, int nl, double *red_gl
     return s;
 }
 
-// Planck table index INT(T*10-499) (code/sfluxi.f90:54-55, code/gfluxi.f90:223-237),
+// Planck table index INT(T*10-499) (code/sfluxi.f90:54-55, code/gfluxi.f90:73-74,86-87),
 // formed without contraction; clamped to the table with a status flag.
 __device__ __forceinline__ int planck_index(double t, uint32_t *status) {
     const double x = __dsub_rn(__dmul_rn(t, 10.0), 499.0);

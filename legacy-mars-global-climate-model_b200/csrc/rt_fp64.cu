@@ -7,16 +7,16 @@
 // Per system the reference calls OPTCV/OPTCI (one column of DTAUK),
 // GETDETAU, then GFLUXV/GFLUXI -> DSOLVER -> DTRIDGL.  Here a system runs:
 //   pass A  top-down over levels: 8-corner k gather and H2O/T/P interpolation
-//           (code/optcv.f90:279-303, code/optci.f90:143-167), cumulative TAUCUM,
+//           (code/optcv.f90:128-176, code/optci.f90:143-167), cumulative TAUCUM,
 //           per-layer DTAU/WBAR and the delta-Eddington scaling
-//           (code/getdetau.f90:308-335 = code/gfluxv.f90:245-272);
+//           (code/getdetau.f90:29-56 = code/gfluxv.f90:76-103);
 //   pass C  bottom-up over layers: two-stream coefficients
-//           (code/gfluxv.f90:277-332, code/gfluxi.f90:219-273), the DSOLVER rows
+//           (code/gfluxv.f90:108-163, code/gfluxi.f90:69-123), the DSOLVER rows
 //           (code/dsolver.f90:54-85) generated in the order DTRIDGL eliminates
-//           them (code/dtridgl.f90:131-138), eliminated on the fly;
-//   pass D  top-down: DTRIDGL back-substitution (code/dtridgl.f90:140-144),
+//           them (code/dtridgl.f90:25-32), eliminated on the fly;
+//   pass D  top-down: DTRIDGL back-substitution (code/dtridgl.f90:34-38),
 //           unmixing (code/dsolver.f90:91-103) and the midpoint fluxes
-//           (code/gfluxv.f90:339-449, code/gfluxi.f90:286-344).
+//           (code/gfluxv.f90:170-280, code/gfluxi.f90:136-194).
 // The flux sums over bands and Gauss points are then formed by one thread
 // per output in the reference's order (code/sfluxv.f90:60-164,
 // code/sfluxi.f90:57-145) and turned into SUNTOT/IRTOTAL/QRAD

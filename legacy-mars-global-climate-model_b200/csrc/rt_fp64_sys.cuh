@@ -460,7 +460,7 @@ __device__ void solve_ir(const SegDev &sg, int c, int nw, int ng, int sidx, ColS
     const double tautop = w.a2[1] * plev[2 - 1] / (plev[4 - 1] - plev[2 - 1]);
     const double btop = (1.0 - mgcm_rt_exp(-tautop / UBARI)) * s.pltop_i[nw - 1];
     const double bsurf = s.bsurf_i[nw - 1];
-    // LAMDA, GAMA, B1, TERM of layer l (code/gfluxi.f90:219-240).  Pass C
+    // LAMDA, GAMA, B1, TERM of layer l (code/gfluxi.f90:69-93).  Pass C
     // and pass D both evaluate them from the pass-A slots (WBARI, DTAUI),
     // which stay intact: recomputing costs less than a round trip of four
     // more per-layer arrays through local memory (measured on the c1 call:

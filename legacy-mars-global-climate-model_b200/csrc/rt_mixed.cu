@@ -3,7 +3,7 @@
 //
 // The visible opacity work -- the 8-corner gather of the k table, the
 // H2O/T/P interpolation and the per-level gas optical depth
-// (code/optcv.f90:279-303) -- runs in FP32 on a table of Cmk*k (k itself
+// (code/optcv.f90:128-176) -- runs in FP32 on a table of Cmk*k (k itself
 // reaches 1e-49, below the FP32 range); the screen kernel does the same.
 // Everything after the per-level optical depth stays FP64: the layer sums,
 // the delta-Eddington scaling, the two-stream coefficients and exponentials,

@@ -7,7 +7,7 @@
 //                 interpolation on the odd ones, GT at the bottom)
 //   QH2O          code/comp3.f:576-589
 //   TAUREF        prescribed dust only: the Conrath profile of
-//                 code/dustprofile.f:88-172 on the PRDST grid, sampled by
+//                 code/dustprofile.f:32-114 on the PRDST grid, sampled by
 //                 code/filltaucum.f:39-55 (JSRCHGT of code/jsrchgt.f90)
 //
 // One warp per column.  The lanes share the exponentials of the dust
@@ -42,12 +42,12 @@ rt_prep(const PrepSeg a) {
     const double ptrop = a.ptrop, rptau = a.rptau;
     if (a.prescribed_dust) {
         if (threadIdx.x == 0) {
-            // code/dustprofile.f:100-104; the exponent is REAL*4 arithmetic
+            // code/dustprofile.f:32-37; the exponent is REAL*4 arithmetic
             const float ex = 1.0f / ((float)PREP_NPDST - 1.0f);
             const double refpr = mgcm_rt_pow(5.0 * a.psf / ptrop, (double)ex);
             prdst[0] = ptrop;
             for (int n = 1; n < PREP_NPDST; ++n) prdst[n] = refpr * prdst[n - 1];
-            // the Fortran DO index where code/dustprofile.f:121-131 leaves its
+            // the Fortran DO index where code/dustprofile.f:59-68 leaves its
             // sum loop: the first n with PRDST(n) >= RPTAU, else NPDST+1
             int ns = PREP_NPDST + 1;
             for (int n = 2; n <= PREP_NPDST; ++n)
@@ -85,7 +85,7 @@ rt_prep(const PrepSeg a) {
                 qrdst0 = tautot / sum;
             }
             qrdst0 = __shfl_sync(full, qrdst0, 0);
-            // QRDST(n), n = 1 .. NPDST-1 (code/dustprofile.f:135-160)
+            // QRDST(n), n = 1 .. NPDST-1 (code/dustprofile.f:79-105)
             for (int n = 1 + lane; n <= PREP_NPDST - 1; n += 32) {
                 double q = 0.0;
                 if (rptau > PR(n + 1)) {
@@ -108,7 +108,7 @@ rt_prep(const PrepSeg a) {
                 QR[n - 1] = q;
             }
             __syncwarp();
-            if (lane == 0) {   // TAUDST (code/dustprofile.f:162-166)
+            if (lane == 0) {   // TAUDST (code/dustprofile.f:109-114)
                 double acc = 0.0;
                 TD[0] = acc;
                 for (int n = 2; n <= PREP_NPDST; ++n) {

@@ -7,10 +7,10 @@
 // midpoint terms -- runs on all four lanes at once.  The parts that are
 // serial in the reference pass through the lanes in order, the carry moving
 // by quad shuffles:
-//   A2  TAUCUM / TAU prefix sums, top-down      (code/optcv.f90:279-303,
-//       code/getdetau.f90:308-335)
-//   C2  DTRIDGL elimination, bottom-up          (code/dtridgl.f90:131-138)
-//   D2  back-substitution and unmixing, top-down (code/dtridgl.f90:140-144,
+//   A2  TAUCUM / TAU prefix sums, top-down      (code/optcv.f90:128-176,
+//       code/getdetau.f90:29-56)
+//   C2  DTRIDGL elimination, bottom-up          (code/dtridgl.f90:25-32)
+//   D2  back-substitution and unmixing, top-down (code/dtridgl.f90:34-38,
 //       code/dsolver.f90:91-103)
 // Every formula keeps the operation order of the one-thread-per-system form
 // in rt_fp64_sys.cuh, so results are bit-identical to it.  All lanes of a

@@ -1,7 +1,7 @@
 // Phase 1 of a column: level bins and per-band opacity terms into shared memory.
-// Restates the set-up loops of code/optcv.f90:240-261,319-359 and
+// Restates the set-up loops of code/optcv.f90:103-124,182-247 and
 // code/optci.f90:113-131,182-220 plus the Planck boundary terms of
-// code/sfluxi.f90:51-62 and code/gfluxi.f90:219-239.
+// code/sfluxi.f90:51-62 and code/gfluxi.f90:69-87.
 #pragma once
 #include "rt_column.cuh"
 
@@ -95,7 +95,7 @@ __device__ inline void stage_band(const SegDev &sg, int c, const RtConst &K,
                 lvl(k + 1, trb, tlb, tcb, gb, gcb);
                 const double cb = (ga * tla + gb * tlb + gca * tca + gcb * tcb) / (tra + trb + tla + tlb + tca + tcb);
                 s.cosb_v[l * D_NV + nw - 1] = cb;
-                s.cbs_v[l * D_NV + nw - 1] = cb / (1.0 + cb);   // code/getdetau.f90:308-335
+                s.cbs_v[l * D_NV + nw - 1] = cb / (1.0 + cb);   // code/getdetau.f90:29-56
                 s.wnum_v[l * D_NV + nw - 1] = tla + tlb + tca + tcb + (tra + trb) * R4(0.9999);
             } else {
                 const int k = LEV;

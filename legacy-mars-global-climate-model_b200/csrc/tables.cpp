@@ -1,8 +1,8 @@
 // Host set-up of the radiation tables, restating the reference RADSETUP chain:
-//   code/setspv.f90:113-151  visible bands, SOLARF (REAL*4 literals), TAURAY
-//   code/setspi.f90:192-259  IR bands and the Planck table (12-point Gauss-Legendre)
+//   code/setspv.f90:67-105  visible bands, SOLARF (REAL*4 literals), TAURAY
+//   code/setspi.f90:70-105  IR bands and the Planck table (12-point Gauss-Legendre)
 //   code/setrad.f90:112-130  PGASREF (REAL*4 literals) and TGASREF
-//   code/laginterp.f90:191-236 log10 of the k records, 4-point Lagrange onto 51 log-p
+//   code/laginterp.f90:71-236 log10 of the k records, 4-point Lagrange onto 51 log-p
 //                            points, 10**ans; code/lagrange.f90:17-31
 // Compiled without FMA contraction so the tables match the reference's x86-64 build.
 #include "tables.h"

@@ -22,7 +22,7 @@ struct HostTables {
     double plimit[NP];
 };
 
-// Reads the two k-coefficient files (code/laginterp.f90:220-230). 0 or <0.
+// Reads the two k-coefficient files (code/laginterp.f90:59-69). 0 or <0.
 int read_ktables(const std::string &dir, std::vector<double> &co2v8, double fzerov[NV],
                  std::vector<double> &co2i8, double fzeroi[NI]);
 

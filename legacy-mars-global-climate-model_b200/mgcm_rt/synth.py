@@ -6,7 +6,7 @@ restatements of the reference routines that build the radiation inputs:
 
 * sigma grid         code/emiss.f:103-115 with DSIG from code/modules.f90:731-737
 * level pressures    code/potemp1.f:95-106, code/fillpt.f90:30-72
-* dust profile       code/dustprofile.f:88-172 (Conrath, CONRNU=0.03, RPTAU=6.1)
+* dust profile       code/dustprofile.f:32-114 (Conrath, CONRNU=0.03, RPTAU=6.1)
                      and code/filltaucum.f:39-55
 * dust optics        code/ini_optdst.f:44-61 with the Wolff constants of
                      code/setrad.f90:73-105
@@ -104,7 +104,7 @@ def _pchip(x, y, xq):
 
 def dust_profile_grid(ptrop: float, psf: float = PSF_TUTORIAL):
     """PRDST and the unit-TAUTOT cumulative optical depth TAUDST/TAUTOT on it
-    (code/dustprofile.f:88-172 with a spatially constant CONRNU)."""
+    (code/dustprofile.f:32-114 with a spatially constant CONRNU)."""
     refpr = (5.0 * psf / ptrop) ** (1.0 / (float(NPDST) - 1.0))
     prdst = np.empty(NPDST)
     prdst[0] = ptrop
@@ -421,7 +421,7 @@ def make_state_batch(ncol: int, L: int = 24, seed: int = 0, active_dust: bool = 
                sigma 0.6) (prescribed dust)
       conr     the Conrath parameter: CONRNU (REAL*4 0.03,
                code/modules.f90:874) or, with vary_conr, U[0.007, 0.04] (the
-               range of the latitude-varying form, code/dustprofile.f:106-114)
+               range of the latitude-varying form, code/dustprofile.f:43-53)
     psf = 7.010 mbar (the tutorial namelist), RPTAU the module's REAL*4 6.1
     (code/modules.f90:854), MWRATIO = MWCO2/MWH2O (code/input.f:180)."""
     b = make_tracer_batch(ncol, L=L, seed=seed, active_dust=active_dust, cloudon=cloudon,

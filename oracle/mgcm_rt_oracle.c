@@ -1463,7 +1463,7 @@ static void aerosols_range(const orc_aero *a, const orc_tracers *t, int c0, int 
 
 /* ------------------------------------------------------------ column prep */
 
-/* code/dustprofile.f:100-104: REFPR = (5.0*PSF/PTROP)**(1.0/(FLOAT(NPDST)-1.0)),
+/* code/dustprofile.f:32-37: REFPR = (5.0*PSF/PTROP)**(1.0/(FLOAT(NPDST)-1.0)),
  * the exponent evaluated in REAL*4; PRDST(1) = PTROP, PRDST(n) = REFPR*PRDST(n-1). */
 void orc_dust_grid(double psf, double ptrop, double *prdst) {
     const float e = 1.0f / ((float)ORC_NPDST - 1.0f);
@@ -1472,7 +1472,7 @@ void orc_dust_grid(double psf, double ptrop, double *prdst) {
     for (int n = 2; n <= ORC_NPDST; ++n) prdst[n - 1] = refpr * prdst[n - 2];
 }
 
-/* code/dustprofile.f:117-170 for one column: the normalising sum of the
+/* code/dustprofile.f:59-114 for one column: the normalising sum of the
  * Conrath profile up to RPTAU, the mixing ratio QRDST per PRDST interval
  * and its running integral TAUDST.  The literals 1. and 1.0 are exact. */
 void orc_dust_profile(const double *prdst, double rptau, double conr, double tautot, double *taudst) {
@@ -1486,7 +1486,7 @@ void orc_dust_profile(const double *prdst, double rptau, double conr, double tau
         }
         if (PR(n) >= rptau) break;
     }
-    /* n = NPDST+1 when the loop ran to its end (code/dustprofile.f:132) */
+    /* n = NPDST+1 when the loop ran to its end (code/dustprofile.f:70-73) */
     {
         const double pave = 0.5 * (rptau + PR(n - 1));
         sum = sum + cexp_(conr * (1.0 - (rptau / pave))) * (rptau - PR(n - 1));

@@ -153,7 +153,7 @@ void orc_dsolflux(const orc_tables *t, int ncol, const double *sol, const double
  *   QH2O                  code/comp3.f:576-589 (MWRATIO * vapour, or the
  *                         REAL*4 1.0E-7 without active water); levels 1-3
  *                         are not set by COMP3 and are 0 here
- *   TAUREF (prescribed)   the Conrath profile of code/dustprofile.f:88-172
+ *   TAUREF (prescribed)   the Conrath profile of code/dustprofile.f:32-114
  *                         on the PRDST grid, sampled by FILLTAUCUM
  *                         (code/filltaucum.f:39-55, JSRCHGT of
  *                         code/jsrchgt.f90)
@@ -170,9 +170,9 @@ typedef struct {
     double *plev, *tlev, *pmid, *tmid, *qh2o; /* [ncol][2L+3] */
     double *tauref;                         /* [ncol][2L+4] (prescribed_dust) */
 } orc_prep_batch;
-/* PRDST(1..NPDST) of code/dustprofile.f:100-104. */
+/* PRDST(1..NPDST) of code/dustprofile.f:32-37. */
 void orc_dust_grid(double psf, double ptrop, double *prdst);
-/* TAUDST(J,I,1..NPDST) of one column (code/dustprofile.f:117-170). */
+/* TAUDST(J,I,1..NPDST) of one column (code/dustprofile.f:59-114). */
 void orc_dust_profile(const double *prdst, double rptau, double conr, double tautot, double *taudst);
 /* JSRCHGT (code/jsrchgt.f90), 1-based result. */
 int orc_jsrchgt(int n, const double *sx, double target);

@@ -274,14 +274,14 @@ def _prep_lib(variant: str = "rt"):
 
 
 def dust_grid(psf: float, ptrop: float) -> np.ndarray:
-    """PRDST(1..NPDST) (code/dustprofile.f:100-104)."""
+    """PRDST(1..NPDST) (code/dustprofile.f:32-37)."""
     out = np.empty(NPDST)
     _prep_lib().orc_dust_grid(psf, ptrop, _p(out))
     return out
 
 
 def dust_profile(prdst, rptau: float, conr: float, tautot: float) -> np.ndarray:
-    """TAUDST(1..NPDST) of one column (code/dustprofile.f:117-170)."""
+    """TAUDST(1..NPDST) of one column (code/dustprofile.f:59-114)."""
     pr = np.ascontiguousarray(prdst, dtype=np.float64)
     out = np.empty(NPDST)
     _prep_lib().orc_dust_profile(_p(pr), rptau, conr, tautot, _p(out))

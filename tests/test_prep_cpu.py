@@ -1,6 +1,6 @@
 """Column prep of the oracle (PL, FILLPT, QH2O, DUSTPROFILE, FILLTAUCUM)
 against independent pure-Python statements of code/potemp1.f:95-106,
-code/fillpt.f90:30-72, code/comp3.f:576-589, code/dustprofile.f:88-172,
+code/fillpt.f90:30-72, code/comp3.f:576-589, code/dustprofile.f:32-114,
 code/filltaucum.f:39-55 and code/jsrchgt.f90 (libm exp/log/pow: agreement
 to 1e-13 relative; the oracle uses the deterministic routines of
 include/mgcm_rt_math.h, which the device uses too)."""
@@ -147,7 +147,7 @@ def test_dust_grid(psf, ptrop):
     assert got[0] == ptrop
     assert np.all(np.diff(got) > 0)
     np.testing.assert_allclose(got, ref, rtol=1e-13, atol=0)
-    # the top of the grid is 5 * PSF (code/dustprofile.f:101) up to the
+    # the top of the grid is 5 * PSF (code/dustprofile.f:32) up to the
     # REAL*4 rounding of the exponent 1/99 (about 1e-8 relative at the top)
     assert abs(got[-1] / (5.0 * psf) - 1.0) < 1e-7
 
