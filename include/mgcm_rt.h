@@ -75,6 +75,9 @@ typedef struct {
     int solver;           /* MGCM_RT_SOLVER_AUTO / _THREAD: one thread per (band, Gauss)
                              system; MGCM_RT_SOLVER_QUAD: four lanes per system with the
                              per-layer values in registers (L <= 51; same results) */
+    int max_queued_jobs;  /* serving: jobs (of <= 32,768 columns) accepted and not yet
+                             finished, at most; a submit beyond it returns MGCM_RT_EBUSY.
+                             0 = 100,000 */
 } mgcm_rt_config;
 
 #define MGCM_RT_SOLVER_AUTO 0
@@ -123,6 +126,8 @@ typedef struct {
     long long systems;      /* two-stream systems solved (after TLIMIT and night skips) */
     int kernels;            /* kernels launched */
     int status;             /* device status word (0 = clean) */
+    long long hbm_used;     /* device bytes the handle's staging arenas hold now */
+    long long hbm_budget;   /* the handle's HBM budget for them */
 } mgcm_rt_stats;
 
 /* Reads CO2H2O_{V,IR}_12_95_INTEL from data_dir (code/laginterp.f90:59-69),
@@ -154,8 +159,12 @@ int mgcm_rt_run_multi(mgcm_rt_handle *h, int nbatch, const mgcm_rt_batch_in *in,
                       mgcm_rt_batch_out *out);
 
 /* Serving: queue a batch (pointers must stay valid until collected), get a
- * ticket.  Requests are admitted against the HBM budget and run
- * concurrently on the device as memory frees up. */
+ * ticket.  Requests are split into jobs of <= 32,768 columns and admitted
+ * onto up to four serving slots as slots and HBM budget free up; a job that
+ * does not fit the budget while others run waits for them (a job that does
+ * not fit an idle device fails with MGCM_RT_ENOMEM).  MGCM_RT_EBUSY when the
+ * request would take the accepted-and-unfinished jobs above
+ * mgcm_rt_config.max_queued_jobs. */
 int mgcm_rt_submit(mgcm_rt_handle *h, const mgcm_rt_batch_in *in, mgcm_rt_batch_out *out,
                    long long *ticket);
 /* 1 = finished (result available), 0 = pending, < 0 = error for the ticket. */
@@ -163,6 +172,23 @@ int mgcm_rt_poll(mgcm_rt_handle *h, long long ticket);
 /* Blocks until the ticket finishes or timeout_s passes (<0: no limit);
  * returns the request's status and releases the ticket. */
 int mgcm_rt_wait(mgcm_rt_handle *h, long long ticket, double timeout_s);
+
+/* Timeline of a request not yet released by mgcm_rt_wait (no counterpart in
+ * the reference, which has no requests).  Host times are ms after the
+ * handle's creation; device times are ms after an event the serving worker
+ * records when it starts, taken from the CUDA events that bracket the
+ * kernels of each of the request's jobs (earliest start, latest end), so
+ * the device intervals of two requests show whether their kernels overlapped.
+ * -1 where not yet known. */
+typedef struct {
+    int done;               /* 1 when every job has finished */
+    int status;             /* request status so far (0 or a negative code) */
+    int jobs;               /* jobs of <= 32,768 columns the request was split into */
+    int deferred;           /* admissions put back because the HBM budget was full */
+    double submit_ms, done_ms;                 /* host */
+    double device_begin_ms, device_end_ms;     /* device */
+} mgcm_rt_request_info;
+int mgcm_rt_get_request_info(mgcm_rt_handle *h, long long ticket, mgcm_rt_request_info *info);
 
 /* ---- tracer inputs: aerosol optics on the device -----------------------
  * The per-level dust and water-ice optical properties that COMP3 builds on
@@ -260,6 +286,18 @@ int mgcm_rt_dsolflux(mgcm_rt_handle *h, int ncol, int device_ptrs, const double 
                      const double *acosz, const double *detau, const double *dndiffv,
                      double *dnvflux);
 
+/* Debug export of the integer bins the device uses (device pointers only:
+ * in->device_ptrs set, outputs device buffers [ncol][LEV], lcoef
+ * [ncol][LEV][4]).  Runs the pipeline's staging kernel on the batch and
+ * reads back, per level K = 2..LEV, the bins of TPINDEX (MT, MP, NH2O) with
+ * WRATIO and LCOEF(1..4) (code/tpindex.f90:72-134, called per level at
+ * code/optcv.f90:107 and code/optci.f90:117), and per level K = 1..LEV the
+ * Planck table index INT(TLEV*10-499) (code/sfluxi.f90:54-55,
+ * code/gfluxi.f90:73-74,86-87).  Level 1 has no TPINDEX call: zeros.
+ * Allocates a temporary staging buffer. */
+int mgcm_rt_debug_bins(mgcm_rt_handle *h, const mgcm_rt_batch_in *in, int *mt, int *mp, int *nh2o,
+                       int *nplanck, double *wratio, double *lcoef);
+
 int mgcm_rt_get_stats(mgcm_rt_handle *h, mgcm_rt_stats *st);
 
 /* Host copies of the set-up tables, laid out as the reference modules hold
@@ -277,12 +315,17 @@ int mgcm_rt_tables_host(const char *data_dir, double *co2v, double *co2i, double
  * outputs are the caller's device buffers (in->device_ptrs must be set).  The
  * call itself allocates nothing: its scratch -- the batch descriptor, the
  * status word and the per-CTA flux staging of the FP64 kernel -- lives in one
- * file-scope static device array of MGCM_RT_NOALLOC_SCRATCH_BYTES that every
- * GPU which loads the library holds until exit.  Runs the FP64 kernel on the
- * handle's stream and waits for it.  Its first call on a device does the
- * set-up: it resolves the array's device address on that device (once per
- * device); make that first call before any stream capture begins.  All calls
- * share the one array, so calls that overlap on the GPU (different threads or
+ * file-scope static device array of MGCM_RT_NOALLOC_SCRATCH_BYTES.  The
+ * array's device address is resolved by mgcm_rt_create on the handle's
+ * device (once per device), so the array is committed on every device that
+ * holds a handle, until the process exits, and the call itself never loads
+ * code or data onto the device.  Always the FP64 kernel: the handle's
+ * precision setting is ignored here.  The handle's validate setting is
+ * honoured (the same NaN/Inf and temperature checks as mgcm_rt_run).  The
+ * grid is capped by the per-CTA staging slabs that fit the array (about 200
+ * at L = 24, 100 at L = 48), so the call is slower than mgcm_rt_run.  Runs on
+ * the handle's stream and waits for it.  All calls share the one array and
+ * each overwrites it, so calls that overlap on the GPU (different threads or
  * handles on the same device) race; serialise them.  Returns MGCM_RT_EINVAL
  * for host pointers and MGCM_RT_ENOMEM if one CTA's staging would not fit. */
 #define MGCM_RT_NOALLOC_SCRATCH_BYTES (16u << 20)

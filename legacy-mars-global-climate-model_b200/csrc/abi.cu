@@ -84,6 +84,11 @@ __global__ void rt_dsolflux_kernel(int ncol, const double *__restrict__ sol,
                                    const double *__restrict__ detau,
                                    const double *__restrict__ dndiffv,
                                    double *__restrict__ dnvflux, const RtConst K);
+__global__ void rt_bins_decode(const SegTable *__restrict__ st, int ncol, int max_nl,
+                               const unsigned char *__restrict__ blocks, size_t stride,
+                               uint32_t *status, int *__restrict__ mt, int *__restrict__ mp,
+                               int *__restrict__ nh, int *__restrict__ npl, double *__restrict__ wr,
+                               double *__restrict__ lk);
 }  // namespace mgcm
 
 using namespace mgcm;
@@ -162,8 +167,12 @@ struct Request {
     std::vector<mgcm_rt_batch_out> out;
     int status = 0;
     int jobs_left = 0;
+    int jobs = 0;          // jobs the request was split into
+    int deferred = 0;      // admissions put back by the HBM budget
     bool done = false;
     std::chrono::steady_clock::time_point t_submit, t_done;
+    // device time of the request's kernels, ms after the handle's epoch event
+    double dev_begin = 1e300, dev_end = -1e300;
 };
 
 struct Job {
@@ -226,6 +235,10 @@ struct mgcm_rt_handle {
     std::vector<std::unique_ptr<Slot>> sslots;
     std::thread worker;
     bool stop = false;
+    int max_jobs = 100000;                          // jobs accepted and not finished, at most
+    int outstanding = 0;
+    cudaEvent_t epoch = nullptr;                    // device time origin of the request timestamps
+    std::chrono::steady_clock::time_point t_epoch;  // host time origin
 };
 
 namespace {
@@ -771,7 +784,10 @@ int run_host(mgcm_rt_handle *h, int nbatch, const mgcm_rt_batch_in *in, mgcm_rt_
                 systems += (long long)*sl.h_nsys;
             }
             const int rc = issue_job(h, sl, sl.stream, in[b], out[b], c0, c1);
-            if (rc) return rc;
+            if (rc) {   // jobs already issued may still copy to or from the caller's buffers
+                for (auto &s : h->slots) cudaStreamSynchronize(s->stream);
+                return rc;
+            }
             used[k & 1] = true;
             nk += sl.kernels;
             cols += c1 - c0;
@@ -1115,7 +1131,10 @@ int run_tracers(mgcm_rt_handle *h, const mgcm_rt_batch_tracers &in, mgcm_rt_batc
             systems += (long long)*sl.h_nsys;
         }
         const int rc = issue_tracer_job(h, sl, sl.stream, in, out, c0, c1, stt);
-        if (rc) return rc;
+        if (rc) {   // jobs already issued may still copy to or from the caller's buffers
+            for (auto &s : h->slots) cudaStreamSynchronize(s->stream);
+            return rc;
+        }
         used[k & 1] = true;
         nk += sl.kernels;
         c0 = c1;
@@ -1166,9 +1185,17 @@ int run_batches(mgcm_rt_handle *h, int nbatch, const mgcm_rt_batch_in *in, mgcm_
 void finish_job(mgcm_rt_handle *h, Slot &sl) {
     std::shared_ptr<Request> r = sl.job.req;
     const int code = status_to_code(*sl.h_status);
+    float b = 0.f, e = 0.f;
+    const bool timed = cudaEventElapsedTime(&b, h->epoch, sl.ev0) == cudaSuccess &&
+                       cudaEventElapsedTime(&e, h->epoch, sl.ev1) == cudaSuccess;
     sl.busy = false;
     sl.job = Job{};
     std::lock_guard<std::mutex> lk(h->qmu);
+    --h->outstanding;
+    if (timed) {
+        r->dev_begin = std::min(r->dev_begin, (double)b);
+        r->dev_end = std::max(r->dev_end, (double)e);
+    }
     if (code && !r->status) r->status = code;
     if (--r->jobs_left == 0) {
         r->done = true;
@@ -1179,6 +1206,7 @@ void finish_job(mgcm_rt_handle *h, Slot &sl) {
 
 void fail_job(mgcm_rt_handle *h, Job &j, int code) {
     std::lock_guard<std::mutex> lk(h->qmu);
+    --h->outstanding;
     if (!j.req->status) j.req->status = code;
     if (--j.req->jobs_left == 0) {
         j.req->done = true;
@@ -1189,6 +1217,7 @@ void fail_job(mgcm_rt_handle *h, Job &j, int code) {
 
 void worker_main(mgcm_rt_handle *h) {
     cudaSetDevice(h->device);
+    cudaEventRecord(h->epoch, nullptr);   // before any job of this worker
     for (;;) {
         bool any_busy = false;
         for (auto &s : h->sslots)
@@ -1222,6 +1251,7 @@ void worker_main(mgcm_rt_handle *h) {
                                      j.c0, j.c1);
             if (rc == MGCM_RT_ENOMEM && any_busy) {   // admitted later, when memory frees up
                 std::lock_guard<std::mutex> lk(h->qmu);
+                ++j.req->deferred;
                 h->jobs.push_front(j);
                 break;
             }
@@ -1277,6 +1307,12 @@ int mgcm_rt_tables_host(const char *data_dir, double *co2v, double *co2i, double
     return MGCM_RT_OK;
 }
 
+}  // extern "C"
+namespace {
+int noalloc_scratch(int device, unsigned char **ptr);
+}  // namespace
+extern "C" {
+
 mgcm_rt_handle *mgcm_rt_create(const mgcm_rt_config *cfg, const char *data_dir, int *status) {
     int dummy;
     if (!status) status = &dummy;
@@ -1291,6 +1327,12 @@ mgcm_rt_handle *mgcm_rt_create(const mgcm_rt_config *cfg, const char *data_dir, 
     cudaDeviceProp prop;
     if (cudaGetDeviceProperties(&prop, h->device) != cudaSuccess) { *status = MGCM_RT_ECUDA; return nullptr; }
     if (const int rc = configure_kernels(h->device)) { *status = rc; return nullptr; }
+    {   // the no-allocation entry point's static scratch: resolve its device
+        // address now, while allocating is allowed, so that loading the
+        // module that holds it never happens inside mgcm_rt_run_noalloc
+        unsigned char *scr = nullptr;
+        if (const int rc = noalloc_scratch(h->device, &scr)) { *status = rc; return nullptr; }
+    }
     if (cfg->solver < MGCM_RT_SOLVER_AUTO || cfg->solver > MGCM_RT_SOLVER_QUAD) { *status = MGCM_RT_EINVAL; return nullptr; }
     h->quad = cfg->solver == MGCM_RT_SOLVER_QUAD;
     h->num_sms = prop.multiProcessorCount;
@@ -1363,6 +1405,10 @@ mgcm_rt_handle *mgcm_rt_create(const mgcm_rt_config *cfg, const char *data_dir, 
                 return fail(MGCM_RT_ENOMEM);
         }
     }
+    if (cfg->max_queued_jobs < 0) return fail(MGCM_RT_EINVAL);
+    if (cfg->max_queued_jobs > 0) h->max_jobs = cfg->max_queued_jobs;
+    if (cudaEventCreate(&h->epoch) != cudaSuccess) return fail(MGCM_RT_ECUDA);
+    h->t_epoch = std::chrono::steady_clock::now();
     size_t freeb = 0, totb = 0;
     cudaMemGetInfo(&freeb, &totb);
     h->budget = cfg->hbm_budget ? cfg->hbm_budget : freeb / 4 * 3;
@@ -1391,6 +1437,7 @@ void mgcm_rt_destroy(mgcm_rt_handle *h) {
     if (h->fork) cudaEventDestroy(h->fork);
     if (h->join0) cudaEventDestroy(h->join0);
     if (h->join1) cudaEventDestroy(h->join1);
+    if (h->epoch) cudaEventDestroy(h->epoch);
     delete h;
 }
 
@@ -1441,6 +1488,9 @@ int mgcm_rt_get_stats(mgcm_rt_handle *h, mgcm_rt_stats *st) {
     if (!h || !st) return MGCM_RT_EINVAL;
     std::lock_guard<std::mutex> lk(h->mu);
     *st = h->stats;
+    std::lock_guard<std::mutex> mk(h->mem_mu);
+    st->hbm_used = (long long)h->used;
+    st->hbm_budget = (long long)h->budget;
     return MGCM_RT_OK;
 }
 
@@ -1477,6 +1527,61 @@ int mgcm_rt_dsolflux(mgcm_rt_handle *h, int ncol, int device_ptrs, const double 
     return MGCM_RT_OK;
 }
 
+int mgcm_rt_debug_bins(mgcm_rt_handle *h, const mgcm_rt_batch_in *in, int *mt, int *mp, int *nh2o,
+                       int *nplanck, double *wratio, double *lcoef) {
+    if (!h || !in || !mt || !mp || !nh2o || !nplanck || !wratio || !lcoef) return MGCM_RT_EINVAL;
+    if (!in->device_ptrs) return MGCM_RT_EINVAL;
+    mgcm_rt_batch_out none{};
+    const int ac = check_args(h, in, &none);
+    if (ac != MGCM_RT_OK && ac != MGCM_RT_EINVAL) return ac;
+    if (in->ncol < 0 || !in->plev || !in->tlev || !in->pmid || !in->tmid || !in->qh2o || !in->tauref ||
+        !in->qextrefdst || !in->qxvdst || !in->sigma || !in->sol)
+        return MGCM_RT_EINVAL;
+    if (in->taurefcld && !in->qextrefcld) return MGCM_RT_EINVAL;
+    if (in->ncol == 0) return MGCM_RT_OK;
+    std::lock_guard<std::mutex> lk(h->mu);
+    if (cudaSetDevice(h->device) != cudaSuccess) return MGCM_RT_ECUDA;
+    if (int rc = finish_pending(h)) return rc;
+    Slot &sl = *h->slots[0];
+    cudaStream_t st = sync_stream(h);
+    const Sizes z = sizes_of(*in);
+    SegDev sd{};
+    sd.ncol = (int)z.ncol;
+    sd.L = z.L;
+    sd.col0 = 0;
+    sd.ptrop = in->ptrop;
+    fill_direct(sd, *in, none);
+    sd.sigma = in->sigma;
+    sd.sol = in->sol;
+    SegTable &tab = *sl.h_segs;
+    tab.nseg = 1;
+    tab.total_cols = (int)z.ncol;
+    tab.seg[0] = sd;
+    size_t stride = 0;
+    pipe_bytes_per_col(z.nl, &stride);
+    unsigned char *blocks = nullptr;
+    if (cudaMalloc(&blocks, z.ncol * stride) != cudaSuccess) return MGCM_RT_ENOMEM;
+    int rc = MGCM_RT_OK;
+    do {
+        if (cudaMemcpyAsync(sl.d_segs, sl.h_segs, offsetof(SegTable, seg) + sizeof(SegDev),
+                            cudaMemcpyHostToDevice, st) ||
+            cudaMemsetAsync(sl.d_status, 0, 256, st)) { rc = MGCM_RT_ECUDA; break; }
+        const int g0 = std::min<int>(((int)z.ncol + 3) / 4, h->num_sms * 4);
+        rt_stage<<<g0, STAGE_THREADS, 0, st>>>(sl.d_segs, 0, (int)z.ncol, z.nl, blocks, stride, h->d_planck,
+                                               h->K, sl.d_status);
+        const long long items = (long long)z.ncol * z.lev;
+        const int g1 = (int)std::min<long long>((items + 255) / 256, (long long)h->num_sms * 8);
+        rt_bins_decode<<<g1, 256, 0, st>>>(sl.d_segs, (int)z.ncol, z.nl, blocks, stride, sl.d_status, mt, mp,
+                                           nh2o, nplanck, wratio, lcoef);
+        if (cudaGetLastError() != cudaSuccess ||
+            cudaMemcpyAsync(sl.h_status, sl.d_status, 4, cudaMemcpyDeviceToHost, st) ||
+            cudaStreamSynchronize(st)) { rc = MGCM_RT_ECUDA; break; }
+        rc = status_to_code(*sl.h_status);
+    } while (0);
+    cudaFree(blocks);
+    return rc;
+}
+
 int mgcm_rt_run_state(mgcm_rt_handle *h, const mgcm_rt_batch_state *in, mgcm_rt_batch_out *out) {
     const int rc = check_state(h, in, out);
     if (rc || in->ncol == 0) return rc;
@@ -1508,8 +1613,11 @@ int mgcm_rt_submit(mgcm_rt_handle *h, const mgcm_rt_batch_in *in, mgcm_rt_batch_
     r->out.push_back(*out);
     r->t_submit = std::chrono::steady_clock::now();
     const int ncol = in->ncol;
+    const int njobs = (ncol + SERVE_JOB_COLS - 1) / SERVE_JOB_COLS;
     std::lock_guard<std::mutex> lk(h->qmu);
-    if (h->jobs.size() > 100000) return MGCM_RT_EBUSY;
+    // queue full: the request's jobs would take the accepted-and-unfinished
+    // jobs above the handle's limit (mgcm_rt_config.max_queued_jobs)
+    if (h->outstanding + njobs > h->max_jobs) return MGCM_RT_EBUSY;
     if (!h->worker.joinable()) {
         h->stop = false;
         h->worker = std::thread(worker_main, h);
@@ -1528,6 +1636,8 @@ int mgcm_rt_submit(mgcm_rt_handle *h, const mgcm_rt_batch_in *in, mgcm_rt_batch_
         j.c0 = c0;
         j.c1 = std::min(ncol, c0 + SERVE_JOB_COLS);
         ++r->jobs_left;
+        ++r->jobs;
+        ++h->outstanding;
         h->jobs.push_back(j);
     }
     h->qcv.notify_all();
@@ -1541,6 +1651,28 @@ int mgcm_rt_poll(mgcm_rt_handle *h, long long ticket) {
     if (it == h->reqs.end()) return MGCM_RT_ENOTFOUND;
     if (!it->second->done) return 0;
     return it->second->status < 0 ? it->second->status : 1;
+}
+
+int mgcm_rt_get_request_info(mgcm_rt_handle *h, long long ticket, mgcm_rt_request_info *info) {
+    if (!h || !info) return MGCM_RT_EINVAL;
+    std::lock_guard<std::mutex> lk(h->qmu);
+    auto it = h->reqs.find(ticket);
+    if (it == h->reqs.end()) return MGCM_RT_ENOTFOUND;
+    const Request &r = *it->second;
+    auto ms = [&](std::chrono::steady_clock::time_point t) {
+        return std::chrono::duration<double, std::milli>(t - h->t_epoch).count();
+    };
+    *info = mgcm_rt_request_info{};
+    info->done = r.done ? 1 : 0;
+    info->status = r.status;
+    info->jobs = r.jobs;
+    info->deferred = r.deferred;
+    info->submit_ms = ms(r.t_submit);
+    info->done_ms = r.done ? ms(r.t_done) : -1.0;
+    const bool dev = r.dev_end >= r.dev_begin;
+    info->device_begin_ms = dev ? r.dev_begin : -1.0;
+    info->device_end_ms = dev ? r.dev_end : -1.0;
+    return MGCM_RT_OK;
 }
 
 int mgcm_rt_wait(mgcm_rt_handle *h, long long ticket, double timeout_s) {
@@ -1834,6 +1966,10 @@ extern "C" int mgcm_rt_run_noalloc(mgcm_rt_handle *h, const mgcm_rt_batch_in *in
                        cudaMemcpyHostToDevice, stream));
     CK(cudaMemsetAsync(d_status, 0, sizeof(uint32_t), stream));
     CK(cudaMemsetAsync(d_nsys, 0, sizeof(unsigned long long), stream));
+    if (h->cfg.validate) {   // the same input checks as the other entry points
+        const int vb = std::min((int)((z.ncol + 255) / 256), h->num_sms * 8);
+        validate_kernel<<<std::max(vb, 1), 256, 0, stream>>>(d_tab, d_status);
+    }
     CK(cudaEventRecord(sl.ev0, stream));
     rt_fp64_kernel<<<grid, BLOCK, smem, stream>>>(d_tab, h->d_kv, h->d_ki, h->d_planck, h->K,
                                                      max_nl, d_status, d_nsys, d_red);
@@ -1850,6 +1986,6 @@ extern "C" int mgcm_rt_run_noalloc(mgcm_rt_handle *h, const mgcm_rt_batch_in *in
     h->stats.columns = (long long)z.ncol;
     h->stats.systems = (long long)ns;
     h->stats.status = (int)st;
-    h->stats.kernels = 1;
+    h->stats.kernels = h->cfg.validate ? 2 : 1;
     return status_to_code(st);
 }

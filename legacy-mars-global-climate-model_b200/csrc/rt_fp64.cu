@@ -590,4 +590,42 @@ __global__ void rt_dsolflux_kernel(int ncol, const double *__restrict__ sol,
     dnvflux[c] = dndiffv[c] + ds;
 }
 
+// Integer bins as the pipeline uses them, for the bit-exact check of
+// tpindex (code/tpindex.f90:72-134) and of the Planck index INT(T*10-499)
+// (code/sfluxi.f90:54-55, code/gfluxi.f90:73-74,86-87).  Reads the column
+// blocks rt_stage wrote -- each level's k-table corner offset and NH2O step
+// -- and turns them back into MT, MP, NH2O; copies WRATIO and LCOEF(1..4);
+// and evaluates planck_index, the function rt_stage uses, on every TLEV.
+// One thread per (column, level K = 1..LEV); outputs [ncol][LEV] (LCOEF
+// [ncol][LEV][4]); level 1 has no tpindex call and gets zeros.
+__global__ void rt_bins_decode(const SegTable *__restrict__ st, int ncol, int max_nl,
+                               const unsigned char *__restrict__ blocks, size_t stride,
+                               uint32_t *status, int *__restrict__ mt, int *__restrict__ mp,
+                               int *__restrict__ nh, int *__restrict__ npl, double *__restrict__ wr,
+                               double *__restrict__ lk) {
+    const SegDev &sg = st->seg[0];
+    const int LEV = 2 * sg.L + 3;
+    const long long n = (long long)ncol * LEV;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int c = (int)(i / LEV), k = (int)(i % LEV) + 1;
+        npl[i] = planck_index(sg.tlev[(size_t)c * LEV + k - 1], status);
+        if (k == 1) {
+            mt[i] = mp[i] = nh[i] = 0;
+            wr[i] = 0.0;
+            for (int q = 0; q < 4; ++q) lk[i * 4 + q] = 0.0;
+            continue;
+        }
+        const ColSmem s = carve_smem(const_cast<unsigned char *>(blocks) + (size_t)c * stride, max_nl,
+                                     nullptr, false);
+        const KLevel &r = s.klev[k];
+        const int e = r.kofs / D_NGK;   // ((MT-1)*NP + MP-1)*NH + NH2O-1
+        nh[i] = e % D_NH + 1;
+        mp[i] = (e / D_NH) % D_NP + 1;
+        mt[i] = e / (D_NH * D_NP) + 1;
+        wr[i] = r.wr;
+        for (int q = 0; q < 4; ++q) lk[i * 4 + q] = r.lk[q];
+    }
+}
+
 }  // namespace mgcm

@@ -29,7 +29,14 @@ _D = C.POINTER(C.c_double)
 
 class Config(C.Structure):
     _fields_ = [("max_layers", C.c_int), ("precision", C.c_int), ("device", C.c_int),
-                ("validate", C.c_int), ("hbm_budget", C.c_size_t), ("solver", C.c_int)]
+                ("validate", C.c_int), ("hbm_budget", C.c_size_t), ("solver", C.c_int),
+                ("max_queued_jobs", C.c_int)]
+
+
+class RequestInfo(C.Structure):
+    _fields_ = [("done", C.c_int), ("status", C.c_int), ("jobs", C.c_int), ("deferred", C.c_int),
+                ("submit_ms", C.c_double), ("done_ms", C.c_double), ("device_begin_ms", C.c_double),
+                ("device_end_ms", C.c_double)]
 
 
 SOLVER_AUTO, SOLVER_THREAD, SOLVER_QUAD = 0, 1, 2
@@ -55,7 +62,8 @@ class BatchOut(C.Structure):
 
 class Stats(C.Structure):
     _fields_ = [("gpu_ms", C.c_double), ("total_ms", C.c_double), ("columns", C.c_longlong),
-                ("systems", C.c_longlong), ("kernels", C.c_int), ("status", C.c_int)]
+                ("systems", C.c_longlong), ("kernels", C.c_int), ("status", C.c_int),
+                ("hbm_used", C.c_longlong), ("hbm_budget", C.c_longlong)]
 
 
 class RTError(RuntimeError):
@@ -110,7 +118,9 @@ def lib():
                                      C.POINTER(C.c_longlong)]
         L.mgcm_rt_poll.argtypes = [C.c_void_p, C.c_longlong]
         L.mgcm_rt_wait.argtypes = [C.c_void_p, C.c_longlong, C.c_double]
+        L.mgcm_rt_get_request_info.argtypes = [C.c_void_p, C.c_longlong, C.POINTER(RequestInfo)]
         L.mgcm_rt_dsolflux.argtypes = [C.c_void_p, C.c_int, C.c_int] + [C.c_void_p] * 5
+        L.mgcm_rt_debug_bins.argtypes = [C.c_void_p, C.POINTER(BatchIn)] + [C.c_void_p] * 6
         L.mgcm_rt_enqueue.argtypes = [C.c_void_p, C.POINTER(BatchIn), C.POINTER(BatchOut)]
         L.mgcm_rt_sync.argtypes = [C.c_void_p]
         L.mgcm_rt_set_stream.argtypes = [C.c_void_p, C.c_void_p]
@@ -188,8 +198,8 @@ class Radiation:
     """A handle on one GPU: tables resident in HBM, runs batches of columns."""
 
     def __init__(self, data_dir, max_layers: int = 48, precision: int = FP64, device: int = 0,
-                 validate: bool = True, hbm_budget: int = 0, solver: int = 0):
-        cfg = Config(max_layers, precision, device, 1 if validate else 0, hbm_budget, solver)
+                 validate: bool = True, hbm_budget: int = 0, solver: int = 0, max_queued_jobs: int = 0):
+        cfg = Config(max_layers, precision, device, 1 if validate else 0, hbm_budget, solver, max_queued_jobs)
         st = C.c_int(0)
         self._h = lib().mgcm_rt_create(C.byref(cfg), str(data_dir).encode(), C.byref(st))
         if not self._h:
@@ -420,6 +430,15 @@ class Radiation:
             raise RTError(rc, "mgcm_rt_poll")
         return rc
 
+    def request_info(self, ticket: int) -> dict:
+        """Timeline of a request not yet released by ``wait`` (host and
+        device ms, jobs, HBM-budget deferrals)."""
+        r = RequestInfo()
+        rc = lib().mgcm_rt_get_request_info(self._h, ticket, C.byref(r))
+        if rc != 0:
+            raise RTError(rc, "mgcm_rt_get_request_info")
+        return {k: getattr(r, k) for k, _ in RequestInfo._fields_}
+
     def wait(self, ticket: int, timeout_s: float = -1.0) -> None:
         rc = lib().mgcm_rt_wait(self._h, ticket, float(timeout_s))
         if rc == -8:
@@ -441,6 +460,24 @@ class Radiation:
                                     *[_ptr(a) for a in args], _ptr(out))
         if rc != 0:
             raise RTError(rc, "mgcm_rt_dsolflux")
+        return out
+
+    def debug_bins(self, b: dict) -> dict:
+        """The integer bins the device stages for batch ``b`` (CUDA tensors):
+        per level K = 1..LEV of each column MT, MP, NH2O, WRATIO, LCOEF(1..4)
+        of TPINDEX (zeros at K = 1) and the Planck index INT(TLEV*10-499)."""
+        import torch
+        keep: list = []
+        bi = make_in(b, True, keep)
+        n, lev = int(b["ncol"]), 2 * int(b["L"]) + 3
+        dev = b["plev"].device
+        out = {k: torch.zeros(n, lev, dtype=torch.int32, device=dev) for k in ("mt", "mp", "nh2o", "nplanck")}
+        out["wratio"] = torch.zeros(n, lev, dtype=torch.float64, device=dev)
+        out["lcoef"] = torch.zeros(n, lev, 4, dtype=torch.float64, device=dev)
+        rc = lib().mgcm_rt_debug_bins(self._h, C.byref(bi), *[out[k].data_ptr() for k in
+                                      ("mt", "mp", "nh2o", "nplanck", "wratio", "lcoef")])
+        if rc != 0:
+            raise RTError(rc, "mgcm_rt_debug_bins")
         return out
 
     def stats(self) -> dict:

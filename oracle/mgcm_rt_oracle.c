@@ -790,6 +790,10 @@ static void gfluxv(int nlay, int lev, double ubar0, double f0pi, double rsf, dou
     }
 }
 
+/* Planck table index NT = T*10.0D0-499 assigned to an INTEGER (truncation
+ * toward zero): code/sfluxi.f90:54-55, code/gfluxi.f90:73-74,86-87. */
+int orc_planck_index(double t) { return (int)(t * 10.0 - 499); }
+
 /* gfluxi.f90:213-344 */
 static void gfluxi(int nlay, const orc_tables *t, const double *tlev, int nw, const double *dtau,
                    const double *taucum, const double *w0, const double *cosbar, double rsf,
@@ -797,8 +801,8 @@ static void gfluxi(int nlay, const orc_tables *t, const double *tlev, int nw, co
     for (int l = 1; l <= nlay - 1; l++) {
         w->alpha[l] = sqrt((1.0 - w0[l]) / (1.0 - w0[l] * cosbar[l]));
         w->lamda[l] = w->alpha[l] * (1.0 - w0[l] * cosbar[l]) / UBARI;
-        int nt2 = (int)(tlev[2 * l + 2 - 1] * 10.0 - 499);
-        int nt = (int)(tlev[2 * l - 1] * 10.0 - 499);
+        int nt2 = orc_planck_index(tlev[2 * l + 2 - 1]);
+        int nt = orc_planck_index(tlev[2 * l - 1]);
         w->b1[l] = (t->planckir[(nt2 - 1) * 5 + nw - 1] - t->planckir[(nt - 1) * 5 + nw - 1]) / dtau[l];
         w->b0[l] = t->planckir[(nt - 1) * 5 + nw - 1];
     }
@@ -806,8 +810,8 @@ static void gfluxi(int nlay, const orc_tables *t, const double *tlev, int nw, co
         int l = nlay;
         w->alpha[l] = sqrt((1.0 - w0[l]) / (1.0 - w0[l] * cosbar[l]));
         w->lamda[l] = w->alpha[l] * (1.0 - w0[l] * cosbar[l]) / UBARI;
-        int nt = (int)(tlev[2 * l + 1 - 1] * 10.0 - 499);
-        int nt2 = (int)(tlev[2 * l - 1] * 10.0 - 499);
+        int nt = orc_planck_index(tlev[2 * l + 1 - 1]);
+        int nt2 = orc_planck_index(tlev[2 * l - 1]);
         w->b1[l] = (t->planckir[(nt - 1) * 5 + nw - 1] - t->planckir[(nt2 - 1) * 5 + nw - 1]) / dtau[l];
         w->b0[l] = t->planckir[(nt2 - 1) * 5 + nw - 1];
     }
@@ -994,8 +998,8 @@ static void column(const orc_tables *t, const orc_batch *b, int col, work_t *w) 
         const double *tlev = c.tlev, *plev = c.plev;
         for (int l = 1; l <= NLAY; l++) fmneti[l - 1] = fluxupi[l - 1] = fluxdni[l - 1] = 0.0;
         double ttop = tlev[2 - 1], tsurf = tlev[LEV - 1];
-        int nts = (int)(tsurf * 10.0 - 499);
-        int ntt = (int)(ttop * 10.0 - 499);
+        int nts = orc_planck_index(tsurf);
+        int ntt = orc_planck_index(ttop);
         double dtau[MAXLAY + 1], wb[MAXLAY + 1], cb[MAXLAY + 1], tci[MAXLEV + 1];
         for (int nw = 1; nw <= 5; nw++) {
             double bsurf = (1.0 - albi) * t->planckir[(nts - 1) * 5 + nw - 1];
@@ -1591,4 +1595,26 @@ void orc_prep(const orc_prep_batch *b) {
         }
         tr[lev1 - 1] = 0.0;
     }
+}
+
+/* Per level of every column: the TPINDEX bins and weights (levels 2..LEV,
+ * as OPTCV/OPTCI call it, code/optcv.f90:103-108, code/optci.f90:113-118;
+ * zeros at level 1) and the Planck index of TLEV (levels 1..LEV).  Outputs
+ * [ncol][LEV]; lcoef [ncol][LEV][4]. */
+void orc_bins_batch(const orc_tables *t, const orc_batch *b, int *mt, int *mp, int *nh2o, int *npl,
+                    double *wratio, double *lcoef) {
+    const int LEV = 2 * b->L + 3;
+    for (int c = 0; c < b->ncol; c++)
+        for (int k = 1; k <= LEV; k++) {
+            const size_t i = (size_t)c * LEV + k - 1;
+            npl[i] = orc_planck_index(b->tlev[i]);
+            if (k == 1) {
+                mt[i] = mp[i] = nh2o[i] = 0;
+                wratio[i] = 0.0;
+                for (int q = 0; q < 4; q++) lcoef[i * 4 + q] = 0.0;
+                continue;
+            }
+            orc_tpindex(t, b->pmid[i], b->tmid[i], b->qh2o[i], &lcoef[i * 4], &mt[i], &mp[i], &nh2o[i],
+                        &wratio[i]);
+        }
 }

@@ -78,6 +78,9 @@ size_t orc_tables_size(void);
 void orc_tpindex(const orc_tables *t, double pw, double tw, double qh2o,
                  double lcoef[4], int *mt, int *mp, int *nh2o, double *wratio);
 
+/* Planck table index INT(T*10-499) (code/sfluxi.f90:54-55). */
+int orc_planck_index(double t);
+
 typedef struct {
     int ncol, L;
     /* inputs */
@@ -142,6 +145,11 @@ typedef struct {
 void orc_aerosols(const orc_aero *a, const orc_tracers *t);
 /* The same over nthreads host threads (<= 0: all). */
 void orc_aerosols_mt(const orc_aero *a, const orc_tracers *t, int nthreads);
+
+/* TPINDEX bins/weights and Planck indices of every level of a batch
+ * ([ncol][LEV], lcoef [ncol][LEV][4]; level 1: zero bins). */
+void orc_bins_batch(const orc_tables *t, const orc_batch *b, int *mt, int *mp, int *nh2o, int *npl,
+                    double *wratio, double *lcoef);
 
 void orc_dsolflux(const orc_tables *t, int ncol, const double *sol, const double *acosz,
                   const double *detau, double *directsol);

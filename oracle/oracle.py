@@ -69,6 +69,7 @@ def lib(variant: str = "rt"):
                                      C.POINTER(C.c_int), _D]
         _lib.orc_optics_column.argtypes = [C.c_void_p, C.POINTER(OrcBatch), C.c_int] + [_D] * 10
         _lib.orc_dsolflux.argtypes = [C.c_void_p, C.c_int, _D, _D, _D, _D]
+        _lib.orc_bins_batch.argtypes = [C.c_void_p, C.POINTER(OrcBatch)] + [C.POINTER(C.c_int)] * 4 + [_D, _D]
         _libs[variant] = _lib
     return _lib
 
@@ -174,6 +175,22 @@ def optics_column(tables: Tables, b: dict, col: int) -> dict:
     lib(tables.variant).orc_optics_column(tables.ptr, C.byref(s), col, *[_p(r[k]) for k in (
         "dtauv", "wbarv", "cosbv", "taucumv", "taugsurfv", "dtaui", "wbari", "cosbi", "taucumi",
         "taugsurfi")])
+    return r
+
+
+def bins_batch(tables: Tables, b: dict) -> dict:
+    """TPINDEX bins and weights and the Planck index of every level of every
+    column (orc_bins_batch): mt, mp, nh2o, nplanck, wratio [ncol][LEV],
+    lcoef [ncol][LEV][4]; level 1 has zero bins."""
+    n, lev = int(b["ncol"]), 2 * int(b["L"]) + 3
+    r = {k: np.zeros((n, lev), dtype=np.int32) for k in ("mt", "mp", "nh2o", "nplanck")}
+    r["wratio"] = np.zeros((n, lev))
+    r["lcoef"] = np.zeros((n, lev, 4))
+    out = alloc_outputs(n, int(b["L"]))
+    s, keep = make_struct(b, out)
+    ip = C.POINTER(C.c_int)
+    lib(tables.variant).orc_bins_batch(tables.ptr, C.byref(s), *[r[k].ctypes.data_as(ip) for k in
+                                       ("mt", "mp", "nh2o", "nplanck")], _p(r["wratio"]), _p(r["lcoef"]))
     return r
 
 

@@ -1,11 +1,13 @@
 """Copy the reference's radiation data files into <repo>/data (git-ignored).
 
-A build step, run by __graft_entry__.build() in the container that holds the
-reference checkout; the copied files then travel with the working tree.  The
-source defaults to the reference checkout's run/data directory.
+A build step: __graft_entry__.build() runs it with the reference checkout's
+run/data directory where that checkout exists; the copied files then travel
+with the working tree.  The source directory is the first argument, else the
+MGCM_RT_REFERENCE_DATA environment variable; with neither, nothing is staged.
 
-    python oracle/stage_data.py [SOURCE_DIR]
+    python oracle/stage_data.py SOURCE_DIR
 """
+import os
 import pathlib
 import shutil
 import sys
@@ -13,11 +15,10 @@ import sys
 FILES = ("CO2H2O_V_12_95_INTEL", "CO2H2O_IR_12_95_INTEL",
          "waterCoated_vis_JD_12bands.dat", "waterCoated_ir_JD_12bands.dat",
          "Dust_vis_wolff2010_JD_12bands.dat", "Dust_ir_wolff2010_JD_12bands.dat")
-DEFAULT_SRC = pathlib.Path("/root/reference/run/data")
 DST = pathlib.Path(__file__).resolve().parents[1] / "data"
 
 
-def stage(src: pathlib.Path = DEFAULT_SRC, dst: pathlib.Path = DST) -> bool:
+def stage(src: pathlib.Path, dst: pathlib.Path = DST) -> bool:
     if not all((src / f).is_file() for f in FILES):
         return False
     dst.mkdir(parents=True, exist_ok=True)
@@ -28,5 +29,6 @@ def stage(src: pathlib.Path = DEFAULT_SRC, dst: pathlib.Path = DST) -> bool:
 
 
 if __name__ == "__main__":
-    ok = stage(pathlib.Path(sys.argv[1]) if len(sys.argv) > 1 else DEFAULT_SRC)
+    src = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("MGCM_RT_REFERENCE_DATA")
+    ok = bool(src) and stage(pathlib.Path(src))
     print("staged" if ok else "source data not found; nothing staged")

@@ -1,7 +1,7 @@
 """Comparison helpers for the parity tests."""
 import numpy as np
 
-from mgcm_rt import OUTPUT_COL, OUTPUT_LAY
+from mgcm_rt import OUTPUT_COL, OUTPUT_LAY, synth
 
 FLUX_LAY = ("fmnetv", "fluxupv", "fluxdnv", "fmneti", "fluxupi", "fluxdni")
 DIV_LAY = ("suntot", "irtotal")
@@ -86,3 +86,31 @@ def mixed_errors(b, got, ref):
     out["heat_dT_Ksol_rms"] = float(np.sqrt(((dth * om) ** 2).mean())) if dth.size else 0.0
     out["heat_dtheta_Ksol_max"] = float(dth.max()) if dth.size else 0.0
     return out
+
+
+def edge_batch(otables):
+    """Columns whose inputs sit on bin edges: pressures at the tpindex
+    limits, temperatures on the 50 K grid and at the Planck table ends,
+    humidity at and beyond the water grid ends, the day threshold."""
+    b = synth.make_batch(12, L=24, seed=12, cloud=True, night_frac=0.0)
+    pref = otables.view()["pfgasref"]
+    lev = b["plev"].shape[1]
+    # pressures: put PMID of some levels exactly at 10**PREF and one ulp off
+    for c, n in enumerate((20, 25, 30, 33)):
+        p = 10.0 ** pref[n]
+        for k in range(4, lev, 7):
+            b["pmid"][c, k] = np.nextafter(p, 0) if k % 2 else p
+    # temperatures exactly on the 50 K grid
+    b["tmid"][4, 3:] = 200.0
+    b["tmid"][5, 3:] = 150.0
+    # Planck ends: T = 50.0 exactly (index 1) on an even level
+    b["tlev"][6, 1] = 50.0
+    b["tlev"][6, 3] = 50.0
+    # water at and above WREFH2O(10), and exactly on interior grid points
+    b["qh2o"][7, 3:] = 0.4
+    b["qh2o"][8, 3:] = 0.7
+    b["qh2o"][9, 3:] = 1.0e-3
+    # day threshold: exactly the REAL*4 1.0e-5 (day) and just below (night)
+    b["acosz"][10] = float(np.float32(1.0e-5))
+    b["acosz"][11] = np.nextafter(float(np.float32(1.0e-5)), 0)
+    return b

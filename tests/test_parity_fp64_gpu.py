@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 import oracle
-from helpers import compare, to_numpy
+from helpers import compare, edge_batch, to_numpy
 from mgcm_rt import abi, synth
 
 pytestmark = pytest.mark.gpu
@@ -50,36 +50,8 @@ def test_device_pointers_match_host(rt, otables):
     check(b, got, ref)
 
 
-def _edge_batch(otables):
-    """Columns whose inputs sit on bin edges: pressures at the tpindex
-    limits, temperatures on the 50 K grid and at the Planck table ends,
-    humidity at and beyond the water grid ends, the day threshold."""
-    b = synth.make_batch(12, L=24, seed=12, cloud=True, night_frac=0.0)
-    pref = otables.view()["pfgasref"]
-    lev = b["plev"].shape[1]
-    # pressures: put PMID of some levels exactly at 10**PREF and one ulp off
-    for c, n in enumerate((20, 25, 30, 33)):
-        p = 10.0 ** pref[n]
-        for k in range(4, lev, 7):
-            b["pmid"][c, k] = np.nextafter(p, 0) if k % 2 else p
-    # temperatures exactly on the 50 K grid
-    b["tmid"][4, 3:] = 200.0
-    b["tmid"][5, 3:] = 150.0
-    # Planck ends: T = 50.0 exactly (index 1) on an even level
-    b["tlev"][6, 1] = 50.0
-    b["tlev"][6, 3] = 50.0
-    # water at and above WREFH2O(10), and exactly on interior grid points
-    b["qh2o"][7, 3:] = 0.4
-    b["qh2o"][8, 3:] = 0.7
-    b["qh2o"][9, 3:] = 1.0e-3
-    # day threshold: exactly the REAL*4 1.0e-5 (day) and just below (night)
-    b["acosz"][10] = float(np.float32(1.0e-5))
-    b["acosz"][11] = np.nextafter(float(np.float32(1.0e-5)), 0)
-    return b
-
-
 def test_edges_match_oracle(rt, otables):
-    b = _edge_batch(otables)
+    b = edge_batch(otables)
     ref = oracle.run_batch(otables, b)
     assert ref["fluxdnv"][11].sum() == 0.0 and ref["fluxdnv"][10].sum() > 0.0
     got = rt.run(b)

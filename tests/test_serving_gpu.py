@@ -74,3 +74,121 @@ def test_layer_counts_alternating_across_slots(data_dir):
             assert max(err.values()) <= 1e-12, err
     finally:
         rt.close()
+
+
+def _served(rt, bd):
+    t, out = rt.submit(bd)
+    return t, out
+
+
+def _wait_done(rt, t, limit_s=60.0):
+    import time
+    t0 = time.monotonic()
+    while rt.poll(t) == 0:
+        assert time.monotonic() - t0 < limit_s, "request did not finish"
+        time.sleep(0.001)
+
+
+def test_requests_overlap_on_the_device(data_dir):
+    """Four one-job requests submitted back to back run on four slots: the
+    device intervals bracketing their kernels (CUDA events) intersect, and
+    each result equals the batch run alone."""
+    rt = abi.Radiation(data_dir, max_layers=24, precision=abi.FP64, validate=False)
+    try:
+        batches = [synth.make_batch(30000, L=24, seed=70 + i, cloud=True) for i in range(4)]
+        alone = [to_numpy(rt.run(b)) for b in batches]
+        tick = [_served(rt, _device(b)) for b in batches]
+        infos = []
+        for t, _ in tick:
+            _wait_done(rt, t)
+            infos.append(rt.request_info(t))
+        for (t, out), b, ref in zip(tick, batches, alone):
+            rt.wait(t, 60.0)
+            err = compare(b, to_numpy(out), ref, 1e-12)
+            assert max(err.values()) <= 1e-12, err
+        iv = sorted((i["device_begin_ms"], i["device_end_ms"]) for i in infos)
+        assert all(b >= 0.0 and e > b for b, e in iv), infos
+        overlaps = sum(1 for a, b in zip(iv, iv[1:]) if b[0] < a[1])
+        assert overlaps >= 1, f"no two requests overlapped on the device: {iv}"
+    finally:
+        rt.close()
+
+
+def test_hbm_budget_defers_admission_then_completes(data_dir):
+    """With an HBM budget that holds one job's staging but not two, the
+    second and third requests wait for the first (their admissions are put
+    back, counted in `deferred`) and still complete with the right results."""
+    n = 30000
+    probe = abi.Radiation(data_dir, max_layers=24, precision=abi.FP64, validate=False)
+    try:
+        batches = [synth.make_batch(n, L=24, seed=80 + i, cloud=True) for i in range(3)]
+        t, _ = _served(probe, _device(batches[0]))
+        probe.wait(t, 60.0)
+        one_job = probe.stats()["hbm_used"]       # one serving slot's arena for n columns
+        alone = [to_numpy(probe.run(b)) for b in batches]
+    finally:
+        probe.close()
+    assert one_job > 0
+    rt = abi.Radiation(data_dir, max_layers=24, precision=abi.FP64, validate=False,
+                       hbm_budget=int(one_job * 1.5))
+    try:
+        tick = [_served(rt, _device(b)) for b in batches]
+        infos = []
+        for t, _ in tick:
+            _wait_done(rt, t)
+            infos.append(rt.request_info(t))
+        for (t, out), b, ref in zip(tick, batches, alone):
+            rt.wait(t, 60.0)
+            err = compare(b, to_numpy(out), ref, 1e-12)
+            assert max(err.values()) <= 1e-12, err
+        assert sum(i["deferred"] for i in infos) >= 1, infos
+        # admitted one at a time: the device intervals do not intersect
+        iv = sorted((i["device_begin_ms"], i["device_end_ms"]) for i in infos)
+        assert all(b[0] >= a[1] for a, b in zip(iv, iv[1:])), iv
+        assert rt.stats()["hbm_used"] <= int(one_job * 1.5)
+    finally:
+        rt.close()
+
+
+def test_queue_full_is_ebusy(data_dir):
+    rt = abi.Radiation(data_dir, max_layers=24, precision=abi.FP64, validate=False, max_queued_jobs=2)
+    try:
+        big = synth.make_batch(3 * 32768, L=24, seed=90, cloud=True)   # 3 jobs: never fits
+        with pytest.raises(abi.RTError) as e:
+            rt.submit(_device(big))
+        assert e.value.code == -9
+        two = synth.make_batch(2 * 32768, L=24, seed=91, cloud=True)   # 2 jobs: fills the queue
+        t, out = rt.submit(_device(two))
+        one = synth.make_batch(100, L=24, seed=92, cloud=True)
+        with pytest.raises(abi.RTError) as e:
+            rt.submit(_device(one))                                    # while both jobs are unfinished
+        assert e.value.code == -9
+        rt.wait(t, 60.0)
+        t2, _ = rt.submit(_device(one))                                # room again
+        rt.wait(t2, 60.0)
+    finally:
+        rt.close()
+
+
+def test_forced_allocation_failure_is_enomem(data_dir):
+    """A one-byte HBM budget: every call that needs staging fails with
+    MGCM_RT_ENOMEM, on the synchronous and the served path, and the library
+    stays usable for a handle with a normal budget."""
+    b = synth.make_batch(500, L=24, seed=93, cloud=True)
+    rt = abi.Radiation(data_dir, max_layers=24, precision=abi.FP64, validate=False, hbm_budget=1)
+    try:
+        for _ in range(2):
+            with pytest.raises(abi.RTError) as e:
+                rt.run(b)
+            assert e.value.code == -5
+        t, _ = rt.submit(_device(b))
+        with pytest.raises(abi.RTError) as e:
+            rt.wait(t, 60.0)
+        assert e.value.code == -5
+    finally:
+        rt.close()
+    ok = abi.Radiation(data_dir, max_layers=24, precision=abi.FP64, validate=False)
+    try:
+        ok.run(b)
+    finally:
+        ok.close()
