@@ -83,6 +83,7 @@ typedef struct {
 #define MGCM_RT_SOLVER_AUTO 0
 #define MGCM_RT_SOLVER_THREAD 1
 #define MGCM_RT_SOLVER_QUAD 2
+#define MGCM_RT_SOLVER_ONCHIP 3   /* one thread per system, per-system arrays on chip */
 
 /* One batch of columns on one vertical grid. */
 typedef struct {

@@ -84,6 +84,11 @@ __global__ void rt_dsolflux_kernel(int ncol, const double *__restrict__ sol,
                                    const double *__restrict__ detau,
                                    const double *__restrict__ dndiffv,
                                    double *__restrict__ dnvflux, const RtConst K);
+template <bool VIS, bool F32, int T>
+__global__ void rt_solve_oc(const SegTable *__restrict__ st, int col_begin, int max_nl,
+                            unsigned char *__restrict__ blocks, size_t stride, const double *__restrict__ ktab,
+                            const float *__restrict__ ktabf, const RtConst K, const int *__restrict__ list,
+                            const unsigned int *count, double *__restrict__ fl, double *__restrict__ sc);
 __global__ void rt_bins_decode(const SegTable *__restrict__ st, int ncol, int max_nl,
                                const unsigned char *__restrict__ blocks, size_t stride,
                                uint32_t *status, int *__restrict__ mt, int *__restrict__ mp,
@@ -96,6 +101,27 @@ using namespace mgcm;
 namespace {
 
 constexpr int BLOCK = 224;
+
+// On-chip solve kernels by family and threads per CTA (rt_onchip.cu).
+using OcKernel = void (*)(const SegTable *__restrict__, int, int, unsigned char *__restrict__, size_t,
+                          const double *__restrict__, const float *__restrict__, const RtConst,
+                          const int *__restrict__, const unsigned int *, double *__restrict__,
+                          double *__restrict__);
+constexpr int OC_NT = 8;   // T = 32, 64, ..., 256
+#define OC_ROW(V, F) {rt_solve_oc<V, F, 32>, rt_solve_oc<V, F, 64>, rt_solve_oc<V, F, 96>,          \
+                       rt_solve_oc<V, F, 128>, rt_solve_oc<V, F, 160>, rt_solve_oc<V, F, 192>,      \
+                       rt_solve_oc<V, F, 224>, rt_solve_oc<V, F, 256>}
+const OcKernel OC_KERNELS[3][OC_NT] = {OC_ROW(true, false), OC_ROW(true, true), OC_ROW(false, false)};
+#undef OC_ROW
+
+// Slots (doubles) per system of a family at NL layers: rt_onchip.cuh.
+int oc_slots(bool vis, int nl) { return vis ? 8 * nl + 1 : 7 * nl; }
+// Largest T (multiple of 32, <= 256) whose slices fit one CTA's shared memory; 0: none.
+int oc_threads(bool vis, int nl) {
+    const size_t per = (size_t)oc_slots(vis, nl) * sizeof(double);
+    const int t = (int)std::min<size_t>(256, SMEM_CAP / per) / 32 * 32;
+    return t;
+}
 constexpr int SYNC_JOB_COLS = 8192;     // columns per job of a synchronous host-buffer call (measured best of 2k-32k)
 #ifndef MGCM_SYNC_RAMP
 #define MGCM_SYNC_RAMP 2048
@@ -215,6 +241,7 @@ struct mgcm_rt_handle {
     double *d_kv = nullptr, *d_ki = nullptr, *d_planck = nullptr;
     float *d_kvf = nullptr;   // FP32 visible table (Cmk*k) of the MIXED path
     bool quad = false;        // four-lane solvers for L <= 51 (mgcm_rt_config.solver)
+    bool onchip = false;      // solvers with the per-system arrays on chip (mgcm_rt_config.solver)
     AeroConst aero{};         // aerosol optics constants (mgcm_rt_run_tracers)
     double *d_mie = nullptr;  // Mie tables on the device; null when the files were absent
     std::mutex mu;                                  // serialises the synchronous API
@@ -447,6 +474,10 @@ int configure_kernels(int device) {
     CK(cudaFuncSetAttribute(rt_fp64_reduce<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_CAP));
     CK(cudaFuncSetAttribute(rt_fp64_reduce<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_CAP));
     CK(cudaFuncSetAttribute(rt_fp64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_CAP));
+    for (int f = 0; f < 3; ++f)
+        for (int q = 0; q < OC_NT; ++q)
+            CK(cudaFuncSetAttribute((const void *)OC_KERNELS[f][q], cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)SMEM_CAP));
     // the solvers use no shared memory: the whole unified L1 goes to the
     // per-system arrays
     for (const void *f : {(const void *)rt_fp64_solve<true>, (const void *)rt_fp64_solve<false>,
@@ -539,7 +570,14 @@ int launch_pipeline(mgcm_rt_handle *h, Slot &sl, cudaStream_t st, int total, int
         CK(cudaStreamWaitEvent(sl.aux, sl.fork_ev, 0));
         cudaStream_t vst = sl.aux;
         const int qr = h->quad ? quad_r_for(max_nl) : 0;
-        if (qr) {
+        const int tv = h->onchip ? oc_threads(true, max_nl) : 0, ti = h->onchip ? oc_threads(false, max_nl) : 0;
+        if (tv > 0 && ti > 0) {
+            const size_t smv = (size_t)tv * oc_slots(true, max_nl) * 8, smi = (size_t)ti * oc_slots(false, max_nl) * 8;
+            OC_KERNELS[mixed ? 1 : 0][tv / 32 - 1]<<<h->num_sms, tv, smv, vst>>>(
+                sl.d_segs, c0, max_nl, blocks, stride, h->d_kv, h->d_kvf, h->K, list_v, counts, fl_v, sc_v);
+            OC_KERNELS[2][ti / 32 - 1]<<<h->num_sms, ti, smi, st>>>(
+                sl.d_segs, c0, max_nl, blocks, stride, h->d_ki, nullptr, h->K, list_i, counts, fl_i, sc_i);
+        } else if (qr) {
             const int gq = h->num_sms * (sl.tune.solve_ctas > 0 ? sl.tune.solve_ctas : sl.occ_quad);
 #define MGCM_QUAD(R)                                                                                        \
     do {                                                                                                    \
@@ -1333,8 +1371,9 @@ mgcm_rt_handle *mgcm_rt_create(const mgcm_rt_config *cfg, const char *data_dir, 
         unsigned char *scr = nullptr;
         if (const int rc = noalloc_scratch(h->device, &scr)) { *status = rc; return nullptr; }
     }
-    if (cfg->solver < MGCM_RT_SOLVER_AUTO || cfg->solver > MGCM_RT_SOLVER_QUAD) { *status = MGCM_RT_EINVAL; return nullptr; }
+    if (cfg->solver < MGCM_RT_SOLVER_AUTO || cfg->solver > MGCM_RT_SOLVER_ONCHIP) { *status = MGCM_RT_EINVAL; return nullptr; }
     h->quad = cfg->solver == MGCM_RT_SOLVER_QUAD;
+    h->onchip = cfg->solver == MGCM_RT_SOLVER_ONCHIP;
     h->num_sms = prop.multiProcessorCount;
     auto fail = [&](int code) { mgcm_rt_destroy(h.release()); *status = code; return nullptr; };
     for (int i = 0; i < 2; ++i) {

@@ -1,0 +1,56 @@
+// Solve kernels of the pipeline with the per-system arrays on chip
+// (rt_onchip.cuh): one thread per kept (band, Gauss) system, T threads per
+// CTA, one CTA per SM holding T slices of 7NL+1 doubles in shared memory.
+// Built with --fmad=false like rt_fp64.cu, so the FP64 forms reproduce the
+// oracle's rounding; the MIXED visible form takes its gas opacities from the
+// FP32 table.
+#include "rt_onchip.cuh"
+
+namespace mgcm {
+
+template <bool VIS, bool F32, int T>
+__global__ void __launch_bounds__(T, 1)
+rt_solve_oc(const SegTable *__restrict__ st, int col_begin, int max_nl, unsigned char *__restrict__ blocks,
+            size_t stride, const double *__restrict__ ktab, const float *__restrict__ ktabf, const RtConst K,
+            const int *__restrict__ list, const unsigned int *count, double *__restrict__ fl,
+            double *__restrict__ sc) {
+    extern __shared__ __align__(16) double oc_slots[];
+    const onchip::SmemSlots<T> ss{oc_slots, (int)threadIdx.x};
+    const unsigned int n = VIS ? count[0] : count[1];
+    for (unsigned int i = blockIdx.x * T + threadIdx.x; i < n; i += gridDim.x * T) {
+        const int e = list[i];
+        const int g = e >> 8, sidx = e & 255;
+        const SegDev &sg = st->seg[find_seg(st, g)];
+        const int c = g - sg.col0;
+        const ColSmem s = carve_smem(blocks + (size_t)(g - col_begin) * stride, max_nl, nullptr, false);
+        double *row = fl + (size_t)i * 2 * max_nl, *scr = sc + (size_t)i * 4;
+        if (VIS) {
+            onchip::solve_vis_oc<onchip::SmemSlots<T>, F32>(sg, c, sidx / D_NG + 1, sidx % D_NG + 1, s, K, ktab,
+                                                            ktabf, ss, row, row + max_nl, scr, scr + 1, scr + 2);
+        } else {
+            const int j = sidx - NSYS_V;
+            onchip::solve_ir_oc(sg, c, j / D_NG + 1, j % D_NG + 1, s, ktab, ss, row, row + max_nl, scr);
+        }
+    }
+}
+
+#define OC_ARGS                                                                                          \
+    const SegTable *__restrict__, int, int, unsigned char *__restrict__, size_t, const double *__restrict__, \
+        const float *__restrict__, const RtConst, const int *__restrict__, const unsigned int *,         \
+        double *__restrict__, double *__restrict__
+#define OC_INST(T)                                                        \
+    template __global__ void rt_solve_oc<true, false, T>(OC_ARGS);       \
+    template __global__ void rt_solve_oc<true, true, T>(OC_ARGS);        \
+    template __global__ void rt_solve_oc<false, false, T>(OC_ARGS);
+OC_INST(32)
+OC_INST(64)
+OC_INST(96)
+OC_INST(128)
+OC_INST(160)
+OC_INST(192)
+OC_INST(224)
+OC_INST(256)
+#undef OC_INST
+#undef OC_ARGS
+
+}  // namespace mgcm

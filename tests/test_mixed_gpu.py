@@ -28,3 +28,17 @@ def test_mixed_within_tolerance(rtm, otables, ncol, L, cloud, seed):
     print(err)
     assert err["flux_max"] <= FLUX_TOL, err
     assert err["heat_dT_Ksol_max"] <= HEAT_TOL, err
+
+
+@pytest.mark.parametrize("L", [24, 48, 99])
+def test_mixed_onchip_solver_within_tolerance(data_dir, otables, L):
+    """MIXED with the on-chip solver form, against the oracle."""
+    b = synth.make_batch(256 if L < 99 else 16, L=L, seed=45 + L, cloud=True)
+    ref = oracle.run_batch(otables, b)
+    rt = abi.Radiation(data_dir, max_layers=L, precision=abi.MIXED, validate=True, solver=abi.SOLVER_ONCHIP)
+    try:
+        err = mixed_errors(b, rt.run(b), ref)
+    finally:
+        rt.close()
+    assert err["flux_max"] <= FLUX_TOL, err
+    assert err["heat_dT_Ksol_max"] <= HEAT_TOL, err
