@@ -539,7 +539,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
-    ap.add_argument("--solver", default="auto", choices=["auto", "thread", "quad", "onchip"],
+    ap.add_argument("--solver", default="auto", choices=["auto", "thread", "quad", "onchip", "tmem"],
                     help="solver form (mgcm_rt_config.solver)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -594,7 +594,8 @@ def main():
         prec = abi.MIXED if pname == "mixed" else abi.FP64
         rt = abi.Radiation(d, max_layers=48, precision=prec, device=local, validate=False,
                            solver={"auto": abi.SOLVER_AUTO, "thread": abi.SOLVER_THREAD,
-                                   "quad": abi.SOLVER_QUAD, "onchip": abi.SOLVER_ONCHIP}[args.solver])
+                                   "quad": abi.SOLVER_QUAD, "onchip": abi.SOLVER_ONCHIP,
+                                   "tmem": abi.SOLVER_TMEM}[args.solver])
         handles[pname] = rt
         outs[pname] = abi.alloc_outputs(ncol, L, device=dev)
         head = pname == precs[-1]   # the headline arm samples clocks

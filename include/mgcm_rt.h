@@ -84,6 +84,7 @@ typedef struct {
 #define MGCM_RT_SOLVER_THREAD 1
 #define MGCM_RT_SOLVER_QUAD 2
 #define MGCM_RT_SOLVER_ONCHIP 3   /* one thread per system, per-system arrays on chip */
+#define MGCM_RT_SOLVER_TMEM 4     /* the same with tensor memory in front of shared memory */
 
 /* One batch of columns on one vertical grid. */
 typedef struct {

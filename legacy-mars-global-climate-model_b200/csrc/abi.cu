@@ -89,6 +89,11 @@ __global__ void rt_solve_oc(const SegTable *__restrict__ st, int col_begin, int 
                             unsigned char *__restrict__ blocks, size_t stride, const double *__restrict__ ktab,
                             const float *__restrict__ ktabf, const RtConst K, const int *__restrict__ list,
                             const unsigned int *count, double *__restrict__ fl, double *__restrict__ sc);
+template <bool VIS, bool F32, int W>
+__global__ void rt_solve_tm(const SegTable *__restrict__ st, int col_begin, int max_nl,
+                            unsigned char *__restrict__ blocks, size_t stride, const double *__restrict__ ktab,
+                            const float *__restrict__ ktabf, const RtConst K, const int *__restrict__ list,
+                            const unsigned int *count, double *__restrict__ fl, double *__restrict__ sc);
 __global__ void rt_bins_decode(const SegTable *__restrict__ st, int ncol, int max_nl,
                                const unsigned char *__restrict__ blocks, size_t stride,
                                uint32_t *status, int *__restrict__ mt, int *__restrict__ mp,
@@ -114,6 +119,7 @@ constexpr int OC_NT = 8;   // T = 32, 64, ..., 256
 const OcKernel OC_KERNELS[3][OC_NT] = {OC_ROW(true, false), OC_ROW(true, true), OC_ROW(false, false)};
 #undef OC_ROW
 
+
 // Slots (doubles) per system of a family at NL layers: rt_onchip.cuh.
 int oc_slots(bool vis, int nl) { return vis ? 8 * nl + 1 : 7 * nl; }
 // Largest T (multiple of 32, <= 256) whose slices fit one CTA's shared memory; 0: none.
@@ -121,6 +127,24 @@ int oc_threads(bool vis, int nl) {
     const size_t per = (size_t)oc_slots(vis, nl) * sizeof(double);
     const int t = (int)std::min<size_t>(256, SMEM_CAP / per) / 32 * 32;
     return t;
+}
+// Tensor-memory forms by family and warps per CTA: W = 4, 6, 8, 9.
+constexpr int TM_NW = 4;
+constexpr int TM_WARPS[TM_NW] = {4, 6, 8, 9};
+#define TM_ROW(V, F) {rt_solve_tm<V, F, 4>, rt_solve_tm<V, F, 6>, rt_solve_tm<V, F, 8>, rt_solve_tm<V, F, 9>}
+const OcKernel TM_KERNELS[3][TM_NW] = {TM_ROW(true, false), TM_ROW(true, true), TM_ROW(false, false)};
+#undef TM_ROW
+// Tensor-memory doubles per thread with W warps (the 512 columns split
+// between the warps of a lane quarter).
+int tm_doubles(int w) { return (int)(((512u / (unsigned)((w + 3) / 4)) & ~1u) / 2); }
+// Index into TM_WARPS of the most warps whose shared-memory remainder fits; -1: none.
+int tm_choice(bool vis, int nl) {
+    for (int q = TM_NW - 1; q >= 0; --q) {
+        const int w = TM_WARPS[q];
+        const long long rest = std::max(0, oc_slots(vis, nl) - tm_doubles(w));
+        if ((size_t)rest * 32 * w * 8 <= SMEM_CAP) return q;
+    }
+    return -1;
 }
 constexpr int SYNC_JOB_COLS = 8192;     // columns per job of a synchronous host-buffer call (measured best of 2k-32k)
 #ifndef MGCM_SYNC_RAMP
@@ -242,6 +266,7 @@ struct mgcm_rt_handle {
     float *d_kvf = nullptr;   // FP32 visible table (Cmk*k) of the MIXED path
     bool quad = false;        // four-lane solvers for L <= 51 (mgcm_rt_config.solver)
     bool onchip = false;      // solvers with the per-system arrays on chip (mgcm_rt_config.solver)
+    bool tmem = false;        // ... with tensor memory in front of shared memory
     AeroConst aero{};         // aerosol optics constants (mgcm_rt_run_tracers)
     double *d_mie = nullptr;  // Mie tables on the device; null when the files were absent
     std::mutex mu;                                  // serialises the synchronous API
@@ -478,6 +503,10 @@ int configure_kernels(int device) {
         for (int q = 0; q < OC_NT; ++q)
             CK(cudaFuncSetAttribute((const void *)OC_KERNELS[f][q], cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)SMEM_CAP));
+    for (int f = 0; f < 3; ++f)
+        for (int q = 0; q < TM_NW; ++q)
+            CK(cudaFuncSetAttribute((const void *)TM_KERNELS[f][q], cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)SMEM_CAP));
     // the solvers use no shared memory: the whole unified L1 goes to the
     // per-system arrays
     for (const void *f : {(const void *)rt_fp64_solve<true>, (const void *)rt_fp64_solve<false>,
@@ -570,8 +599,26 @@ int launch_pipeline(mgcm_rt_handle *h, Slot &sl, cudaStream_t st, int total, int
         CK(cudaStreamWaitEvent(sl.aux, sl.fork_ev, 0));
         cudaStream_t vst = sl.aux;
         const int qr = h->quad ? quad_r_for(max_nl) : 0;
-        const int tv = h->onchip ? oc_threads(true, max_nl) : 0, ti = h->onchip ? oc_threads(false, max_nl) : 0;
-        if (tv > 0 && ti > 0) {
+        const bool oc = h->onchip || h->tmem;
+        const int tv = oc ? oc_threads(true, max_nl) : 0, ti = oc ? oc_threads(false, max_nl) : 0;
+        // tensor-memory forms: every system of the launch on one layer count
+        bool one_l = true;
+        for (int q = 1; q < sl.h_segs->nseg; ++q) one_l = one_l && sl.h_segs->seg[q].L == sl.h_segs->seg[0].L;
+        const int qv = h->tmem && one_l ? tm_choice(true, max_nl) : -1;
+        const int qi = h->tmem && one_l ? tm_choice(false, max_nl) : -1;
+        if (qv >= 0 && qi >= 0) {
+            const int wv = TM_WARPS[qv], wi = TM_WARPS[qi];
+            // at least 116 KB of shared memory each: no two CTAs that hold the
+            // SM's 512 TMEM columns ever share an SM (a second allocation
+            // would wait for the first CTA to finish)
+            const size_t floor_b = 116 * 1024;
+            const size_t smv = std::max(floor_b, (size_t)std::max(0, oc_slots(true, max_nl) - tm_doubles(wv)) * 32 * wv * 8);
+            const size_t smi = std::max(floor_b, (size_t)std::max(0, oc_slots(false, max_nl) - tm_doubles(wi)) * 32 * wi * 8);
+            TM_KERNELS[mixed ? 1 : 0][qv]<<<h->num_sms, 32 * wv, smv, vst>>>(
+                sl.d_segs, c0, max_nl, blocks, stride, h->d_kv, h->d_kvf, h->K, list_v, counts, fl_v, sc_v);
+            TM_KERNELS[2][qi]<<<h->num_sms, 32 * wi, smi, st>>>(
+                sl.d_segs, c0, max_nl, blocks, stride, h->d_ki, nullptr, h->K, list_i, counts, fl_i, sc_i);
+        } else if (tv > 0 && ti > 0) {
             const size_t smv = (size_t)tv * oc_slots(true, max_nl) * 8, smi = (size_t)ti * oc_slots(false, max_nl) * 8;
             OC_KERNELS[mixed ? 1 : 0][tv / 32 - 1]<<<h->num_sms, tv, smv, vst>>>(
                 sl.d_segs, c0, max_nl, blocks, stride, h->d_kv, h->d_kvf, h->K, list_v, counts, fl_v, sc_v);
@@ -1371,7 +1418,8 @@ mgcm_rt_handle *mgcm_rt_create(const mgcm_rt_config *cfg, const char *data_dir, 
         unsigned char *scr = nullptr;
         if (const int rc = noalloc_scratch(h->device, &scr)) { *status = rc; return nullptr; }
     }
-    if (cfg->solver < MGCM_RT_SOLVER_AUTO || cfg->solver > MGCM_RT_SOLVER_ONCHIP) { *status = MGCM_RT_EINVAL; return nullptr; }
+    if (cfg->solver < MGCM_RT_SOLVER_AUTO || cfg->solver > MGCM_RT_SOLVER_TMEM) { *status = MGCM_RT_EINVAL; return nullptr; }
+    h->tmem = cfg->solver == MGCM_RT_SOLVER_TMEM;
     h->quad = cfg->solver == MGCM_RT_SOLVER_QUAD;
     h->onchip = cfg->solver == MGCM_RT_SOLVER_ONCHIP;
     h->num_sms = prop.multiProcessorCount;

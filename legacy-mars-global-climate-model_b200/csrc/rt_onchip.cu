@@ -34,6 +34,55 @@ rt_solve_oc(const SegTable *__restrict__ st, int col_begin, int max_nl, unsigned
     }
 }
 
+// The same with tensor memory in front of shared memory: W warps, one CTA
+// per SM, the CTA's 512 TMEM columns split between the warps that share a
+// lane quarter (warps w and w+4, w+8, ...), vt doubles per thread.  Loops
+// are warp-uniform: every warp takes 32 consecutive list entries; lanes past
+// the end repeat the last entry (identical values to the same rows).  All
+// systems of the launch have one layer count (the host checks), so the
+// per-system loops run the same trips on every lane.
+template <bool VIS, bool F32, int W>
+__global__ void __launch_bounds__(32 * W, 1)
+rt_solve_tm(const SegTable *__restrict__ st, int col_begin, int max_nl, unsigned char *__restrict__ blocks,
+            size_t stride, const double *__restrict__ ktab, const float *__restrict__ ktabf, const RtConst K,
+            const int *__restrict__ list, const unsigned int *count, double *__restrict__ fl,
+            double *__restrict__ sc) {
+    constexpr int T = 32 * W;
+    constexpr int GROUPS = (W + 3) / 4;
+    constexpr uint32_t COLS = (512 / GROUPS) & ~1u;   // TMEM columns per thread
+    extern __shared__ __align__(16) double oc_slots[];
+    __shared__ uint32_t tm_base;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (warp == 0) tmem_alloc(&tm_base, 512);
+    tmem_fence_before_sync();
+    __syncthreads();
+    tmem_fence_after_sync();
+    const uint32_t taddr = tm_base + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(warp >> 2) * COLS;
+    const onchip::HybridSlots<T> ss{oc_slots, (int)threadIdx.x, taddr, (int)(COLS / 2)};
+    const unsigned int n = VIS ? count[0] : count[1];
+    for (unsigned int base = blockIdx.x * T + 32 * warp; base < n; base += gridDim.x * T) {
+        const unsigned int i = min(base + lane, n - 1);
+        const int e = list[i];
+        const int g = e >> 8, sidx = e & 255;
+        const SegDev &sg = st->seg[find_seg(st, g)];
+        const int c = g - sg.col0;
+        const ColSmem s = carve_smem(blocks + (size_t)(g - col_begin) * stride, max_nl, nullptr, false);
+        double *row = fl + (size_t)i * 2 * max_nl, *scr = sc + (size_t)i * 4;
+        if (VIS) {
+            onchip::solve_vis_oc<onchip::HybridSlots<T>, F32>(sg, c, sidx / D_NG + 1, sidx % D_NG + 1, s, K,
+                                                              ktab, ktabf, ss, row, row + max_nl, scr, scr + 1,
+                                                              scr + 2);
+        } else {
+            const int j = sidx - NSYS_V;
+            onchip::solve_ir_oc(sg, c, j / D_NG + 1, j % D_NG + 1, s, ktab, ss, row, row + max_nl, scr);
+        }
+    }
+    tmem_fence_before_sync();
+    __syncthreads();
+    tmem_fence_after_sync();
+    if (warp == 0) tmem_dealloc(tm_base, 512);
+}
+
 #define OC_ARGS                                                                                          \
     const SegTable *__restrict__, int, int, unsigned char *__restrict__, size_t, const double *__restrict__, \
         const float *__restrict__, const RtConst, const int *__restrict__, const unsigned int *,         \
@@ -51,6 +100,15 @@ OC_INST(192)
 OC_INST(224)
 OC_INST(256)
 #undef OC_INST
+#define TM_INST(W)                                                        \
+    template __global__ void rt_solve_tm<true, false, W>(OC_ARGS);       \
+    template __global__ void rt_solve_tm<true, true, W>(OC_ARGS);        \
+    template __global__ void rt_solve_tm<false, false, W>(OC_ARGS);
+TM_INST(4)
+TM_INST(6)
+TM_INST(8)
+TM_INST(9)
+#undef TM_INST
 #undef OC_ARGS
 
 }  // namespace mgcm

@@ -23,6 +23,7 @@
 //  code/dtridgl.f90:25-38).
 #pragma once
 #include "rt_fp64_sys.cuh"
+#include "rt_tmem.cuh"
 
 namespace mgcm {
 namespace onchip {
@@ -40,6 +41,26 @@ struct SmemSlots {
     int t;
     __device__ __forceinline__ double get(int v) const { return base[v * T + t]; }
     __device__ __forceinline__ void put(int v, double x) const { base[v * T + t] = x; }
+};
+
+// Tensor memory first, shared memory beyond: value v < vt at two TMEM
+// columns of the thread's lane (taddr + 2v), the rest at sbase[(v - vt) * T
+// + t].  Every get/put is executed by all 32 threads of the warp with the
+// same v (the solves' loops are warp-uniform when the warp's systems share
+// one layer count).
+template <int T>
+struct HybridSlots {
+    double *sbase;
+    int t;
+    uint32_t taddr;
+    int vt;
+    __device__ __forceinline__ double get(int v) const {
+        return v < vt ? tmem_get(taddr + 2u * (uint32_t)v) : sbase[(v - vt) * T + t];
+    }
+    __device__ __forceinline__ void put(int v, double x) const {
+        if (v < vt) tmem_put(taddr + 2u * (uint32_t)v, x);
+        else sbase[(v - vt) * T + t] = x;
+    }
 };
 
 // ---------------------------------------------------------------- infrared

@@ -40,6 +40,7 @@ __device__ __forceinline__ void tmem_fence_after_sync() {
 
 // One double per thread at taddr (two columns), store and wait.
 __device__ __forceinline__ void tmem_put(uint32_t taddr, double x) {
+    __syncwarp();   // the .sync.aligned forms need the whole warp converged
     const uint32_t lo = (uint32_t)__double2loint(x), hi = (uint32_t)__double2hiint(x);
     asm volatile(
         "tcgen05.st.sync.aligned.32x32b.x2.b32 [%0], {%1, %2};\n"
@@ -51,6 +52,7 @@ __device__ __forceinline__ void tmem_put(uint32_t taddr, double x) {
 // One double per thread from taddr, load and wait (the registers are only
 // defined after the wait, so both sit in one statement).
 __device__ __forceinline__ double tmem_get(uint32_t taddr) {
+    __syncwarp();
     uint32_t lo, hi;
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x2.b32 {%0, %1}, [%2];\n"
@@ -63,6 +65,7 @@ __device__ __forceinline__ double tmem_get(uint32_t taddr) {
 
 // Four doubles from taddr (eight columns) with one wait.
 __device__ __forceinline__ void tmem_get4(uint32_t taddr, double &a, double &b, double &c, double &d) {
+    __syncwarp();
     uint32_t r[8];
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];\n"

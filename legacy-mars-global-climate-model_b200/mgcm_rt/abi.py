@@ -39,7 +39,7 @@ class RequestInfo(C.Structure):
                 ("device_end_ms", C.c_double)]
 
 
-SOLVER_AUTO, SOLVER_THREAD, SOLVER_QUAD, SOLVER_ONCHIP = 0, 1, 2, 3
+SOLVER_AUTO, SOLVER_THREAD, SOLVER_QUAD, SOLVER_ONCHIP, SOLVER_TMEM = 0, 1, 2, 3, 4
 
 
 _IN_PTRS = ("sigma", "sol", "plev", "tlev", "pmid", "tmid", "qh2o", "tauref", "qextrefdst",
