@@ -137,12 +137,15 @@ const OcKernel TM_KERNELS[3][TM_NW] = {TM_ROW(true, false), TM_ROW(true, true), 
 // Tensor-memory doubles per thread with W warps (the 512 columns split
 // between the warps of a lane quarter).
 int tm_doubles(int w) { return (int)(((512u / (unsigned)((w + 3) / 4)) & ~1u) / 2); }
+// Dynamic shared memory the tensor-memory forms may take: the cap less room
+// for their static shared memory (the TMEM address word).
+constexpr size_t TM_SMEM_CAP = SMEM_CAP - 1024;
 // Index into TM_WARPS of the most warps whose shared-memory remainder fits; -1: none.
 int tm_choice(bool vis, int nl) {
     for (int q = TM_NW - 1; q >= 0; --q) {
         const int w = TM_WARPS[q];
         const long long rest = std::max(0, oc_slots(vis, nl) - tm_doubles(w));
-        if ((size_t)rest * 32 * w * 8 <= SMEM_CAP) return q;
+        if ((size_t)rest * 32 * w * 8 <= TM_SMEM_CAP) return q;
     }
     return -1;
 }
@@ -506,7 +509,7 @@ int configure_kernels(int device) {
     for (int f = 0; f < 3; ++f)
         for (int q = 0; q < TM_NW; ++q)
             CK(cudaFuncSetAttribute((const void *)TM_KERNELS[f][q], cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)SMEM_CAP));
+                                    (int)TM_SMEM_CAP));
     // the solvers use no shared memory: the whole unified L1 goes to the
     // per-system arrays
     for (const void *f : {(const void *)rt_fp64_solve<true>, (const void *)rt_fp64_solve<false>,
@@ -1417,6 +1420,26 @@ mgcm_rt_handle *mgcm_rt_create(const mgcm_rt_config *cfg, const char *data_dir, 
         // module that holds it never happens inside mgcm_rt_run_noalloc
         unsigned char *scr = nullptr;
         if (const int rc = noalloc_scratch(h->device, &scr)) { *status = rc; return nullptr; }
+    }
+    {   // The solve kernels keep per-system arrays in local memory, and the
+        // driver grows a context's local-memory pool at the first launch
+        // that needs more (about 2 GB here).  Reserve it now, while
+        // allocating is allowed, through the per-thread stack limit, so that
+        // no later call -- mgcm_rt_run_noalloc in particular -- allocates.
+        size_t need = 0, cur = 0;
+        for (const void *f : {(const void *)rt_fp64_kernel, (const void *)rt_fp64_solve<true>,
+                              (const void *)rt_fp64_solve<false>, (const void *)rt_mixed_solve_vis,
+                              (const void *)rt_fp64_screen<false>, (const void *)rt_fp64_screen<true>}) {
+            cudaFuncAttributes fa{};
+            if (cudaFuncGetAttributes(&fa, f) != cudaSuccess) { *status = MGCM_RT_ECUDA; return nullptr; }
+            need = std::max(need, (size_t)fa.localSizeBytes);
+        }
+        need = (need + 1024 + 15) / 16 * 16;
+        if (cudaDeviceGetLimit(&cur, cudaLimitStackSize) != cudaSuccess) { *status = MGCM_RT_ECUDA; return nullptr; }
+        if (cur < need && cudaDeviceSetLimit(cudaLimitStackSize, need) != cudaSuccess) {
+            *status = MGCM_RT_ENOMEM;
+            return nullptr;
+        }
     }
     if (cfg->solver < MGCM_RT_SOLVER_AUTO || cfg->solver > MGCM_RT_SOLVER_TMEM) { *status = MGCM_RT_EINVAL; return nullptr; }
     h->tmem = cfg->solver == MGCM_RT_SOLVER_TMEM;

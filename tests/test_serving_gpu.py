@@ -97,7 +97,8 @@ def test_requests_overlap_on_the_device(data_dir):
     try:
         batches = [synth.make_batch(30000, L=24, seed=70 + i, cloud=True) for i in range(4)]
         alone = [to_numpy(rt.run(b)) for b in batches]
-        tick = [_served(rt, _device(b)) for b in batches]
+        dev = [_device(b) for b in batches]       # on the device before the first submit
+        tick = [_served(rt, d) for d in dev]      # back to back
         infos = []
         for t, _ in tick:
             _wait_done(rt, t)
@@ -132,7 +133,8 @@ def test_hbm_budget_defers_admission_then_completes(data_dir):
     rt = abi.Radiation(data_dir, max_layers=24, precision=abi.FP64, validate=False,
                        hbm_budget=int(one_job * 1.5))
     try:
-        tick = [_served(rt, _device(b)) for b in batches]
+        dev = [_device(b) for b in batches]
+        tick = [_served(rt, d) for d in dev]
         infos = []
         for t, _ in tick:
             _wait_done(rt, t)
@@ -157,14 +159,14 @@ def test_queue_full_is_ebusy(data_dir):
         with pytest.raises(abi.RTError) as e:
             rt.submit(_device(big))
         assert e.value.code == -9
-        two = synth.make_batch(2 * 32768, L=24, seed=91, cloud=True)   # 2 jobs: fills the queue
-        t, out = rt.submit(_device(two))
-        one = synth.make_batch(100, L=24, seed=92, cloud=True)
+        two = _device(synth.make_batch(2 * 32768, L=24, seed=91, cloud=True))   # 2 jobs: fills the queue
+        one = _device(synth.make_batch(100, L=24, seed=92, cloud=True))
+        t, out = rt.submit(two)
         with pytest.raises(abi.RTError) as e:
-            rt.submit(_device(one))                                    # while both jobs are unfinished
+            rt.submit(one)                                             # while both jobs are unfinished
         assert e.value.code == -9
         rt.wait(t, 60.0)
-        t2, _ = rt.submit(_device(one))                                # room again
+        t2, _ = rt.submit(one)                                         # room again
         rt.wait(t2, 60.0)
     finally:
         rt.close()
