@@ -62,6 +62,10 @@ WORKLOADS = {
 }
 
 
+# mgcm_rt_config.solver by --solver name
+SOLVERS = {"auto": 0, "thread": 1, "quad": 2, "onchip": 3, "tmem": 4, "fused": 5}
+
+
 def algorithmic_bytes_per_column(L: int, cloud: bool) -> int:
     """Bytes the C ABI moves per column (FP64): inputs, outputs, DETAU and
     CUMTAUV in and out (both are in/out arrays of the ABI).  8*(171L+815) with
@@ -453,7 +457,8 @@ def run_ensemble(args, wl):
     clk_summary = None
     for pname in ("fp64", "mixed"):
         prec = abi.MIXED if pname == "mixed" else abi.FP64
-        rt = abi.Radiation(d, max_layers=48, precision=prec, validate=False, hbm_budget=48 << 30)
+        rt = abi.Radiation(d, max_layers=48, precision=prec, validate=False, hbm_budget=48 << 30,
+                           solver=SOLVERS[args.solver])
         g = rt.graph(members, autotune=True)
         info = g.info()
         for _ in range(args.warmup):
@@ -539,7 +544,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
-    ap.add_argument("--solver", default="auto", choices=["auto", "thread", "quad", "onchip", "tmem"],
+    ap.add_argument("--solver", default="auto", choices=["auto", "thread", "quad", "onchip", "tmem", "fused"],
                     help="solver form (mgcm_rt_config.solver)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -593,9 +598,7 @@ def main():
     for pname in precs:
         prec = abi.MIXED if pname == "mixed" else abi.FP64
         rt = abi.Radiation(d, max_layers=48, precision=prec, device=local, validate=False,
-                           solver={"auto": abi.SOLVER_AUTO, "thread": abi.SOLVER_THREAD,
-                                   "quad": abi.SOLVER_QUAD, "onchip": abi.SOLVER_ONCHIP,
-                                   "tmem": abi.SOLVER_TMEM}[args.solver])
+                           solver=SOLVERS[args.solver])
         handles[pname] = rt
         outs[pname] = abi.alloc_outputs(ncol, L, device=dev)
         head = pname == precs[-1]   # the headline arm samples clocks

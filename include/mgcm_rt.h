@@ -85,6 +85,8 @@ typedef struct {
 #define MGCM_RT_SOLVER_QUAD 2
 #define MGCM_RT_SOLVER_ONCHIP 3   /* one thread per system, per-system arrays on chip */
 #define MGCM_RT_SOLVER_TMEM 4     /* the same with tensor memory in front of shared memory */
+#define MGCM_RT_SOLVER_FUSED 5    /* one persistent kernel per call: stage, screen, solve and
+                                     reduce per tile of columns (thread-per-system solves) */
 
 /* One batch of columns on one vertical grid. */
 typedef struct {
@@ -262,8 +264,9 @@ int mgcm_rt_run_state(mgcm_rt_handle *h, const mgcm_rt_batch_state *in, mgcm_rt_
  * arrays it was created with must stay allocated. */
 typedef struct mgcm_rt_graph mgcm_rt_graph;
 typedef struct mgcm_rt_tune {
-    int chunk_cols;        /* columns per pipeline pass */
-    int solve_ctas_per_sm; /* solver CTAs per SM (0 = as many as fit) */
+    int chunk_cols;        /* columns per pipeline pass (fused form: columns per tile) */
+    int solve_ctas_per_sm; /* solver CTAs per SM (0 = as many as fit; fused form: CTAs per SM
+                              the register budget allows) */
     int reduce_rows;       /* kept-system rows per TMA chunk of the reduce */
     int candidates;        /* launch shapes timed by the autotuner */
     int tuning_cols;       /* columns of the tuning sample */
@@ -271,6 +274,7 @@ typedef struct mgcm_rt_tune {
     double best_ms;        /* chosen shape on the sample */
     int kernels;           /* kernel launches in the captured graph */
     int columns;           /* columns of all batches */
+    int threads_per_cta;   /* fused form: threads per CTA (0 for the pipeline) */
 } mgcm_rt_tune;
 int mgcm_rt_graph_create(mgcm_rt_handle *h, int nbatch, const mgcm_rt_batch_in *in,
                          mgcm_rt_batch_out *out, int autotune, mgcm_rt_graph **graph);
@@ -320,8 +324,9 @@ int mgcm_rt_tables_host(const char *data_dir, double *co2v, double *co2i, double
  * file-scope static device array of MGCM_RT_NOALLOC_SCRATCH_BYTES.  The
  * array's device address is resolved by mgcm_rt_create on the handle's
  * device (once per device), so the array is committed on every device that
- * holds a handle, until the process exits, and the call itself never loads
- * code or data onto the device.  Always the FP64 kernel: the handle's
+ * holds a handle, until the process exits.  mgcm_rt_create also reserves the
+ * local memory the kernels need (the per-thread stack limit), so the call
+ * itself never loads code or grows a device memory pool.  Always the FP64 kernel: the handle's
  * precision setting is ignored here.  The handle's validate setting is
  * honoured (the same NaN/Inf and temperature checks as mgcm_rt_run).  The
  * grid is capped by the per-CTA staging slabs that fit the array (about 200

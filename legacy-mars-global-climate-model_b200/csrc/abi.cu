@@ -94,6 +94,14 @@ __global__ void rt_solve_tm(const SegTable *__restrict__ st, int col_begin, int 
                             unsigned char *__restrict__ blocks, size_t stride, const double *__restrict__ ktab,
                             const float *__restrict__ ktabf, const RtConst K, const int *__restrict__ list,
                             const unsigned int *count, double *__restrict__ fl, double *__restrict__ sc);
+template <bool F32, int TC, int THREADS, int MINB>
+__global__ void rt_fused(const SegTable *__restrict__ st, int ncols, int max_nl, unsigned char *__restrict__ scratch,
+                         size_t cta_bytes, size_t stride, const double *__restrict__ kv,
+                         const double *__restrict__ ki, const float *__restrict__ kvf,
+                         const double *__restrict__ planck, const RtConst K, unsigned int *tile_ctr,
+                         uint32_t *status, unsigned long long *nsys);
+size_t fused_smem(int warps, int tc);
+size_t fused_scratch_per_cta(int tc, int max_nl, size_t stride);
 __global__ void rt_bins_decode(const SegTable *__restrict__ st, int ncol, int max_nl,
                                const unsigned char *__restrict__ blocks, size_t stride,
                                uint32_t *status, int *__restrict__ mt, int *__restrict__ mp,
@@ -119,6 +127,21 @@ constexpr int OC_NT = 8;   // T = 32, 64, ..., 256
 const OcKernel OC_KERNELS[3][OC_NT] = {OC_ROW(true, false), OC_ROW(true, true), OC_ROW(false, false)};
 #undef OC_ROW
 
+
+// Persistent fused kernel (rt_fused.cu) by precision and launch shape.
+using FusedKernel = void (*)(const SegTable *__restrict__, int, int, unsigned char *__restrict__, size_t, size_t,
+                             const double *__restrict__, const double *__restrict__, const float *__restrict__,
+                             const double *__restrict__, const RtConst, unsigned int *, uint32_t *,
+                             unsigned long long *);
+struct FusedShape { int tc, threads, minb; };
+constexpr int FUSED_NS = 6;
+constexpr FusedShape FUSED_SHAPES[FUSED_NS] = {{2, 128, 8}, {4, 128, 8}, {8, 128, 8},
+                                               {4, 128, 6}, {4, 256, 4}, {8, 256, 4}};
+constexpr int FUSED_DEFAULT = 1;
+#define FZ_ROW(F) {rt_fused<F, 2, 128, 8>, rt_fused<F, 4, 128, 8>, rt_fused<F, 8, 128, 8>, \
+                   rt_fused<F, 4, 128, 6>, rt_fused<F, 4, 256, 4>, rt_fused<F, 8, 256, 4>}
+const FusedKernel FUSED_KERNELS[2][FUSED_NS] = {FZ_ROW(false), FZ_ROW(true)};
+#undef FZ_ROW
 
 // Slots (doubles) per system of a family at NL layers: rt_onchip.cuh.
 int oc_slots(bool vis, int nl) { return vis ? 8 * nl + 1 : 7 * nl; }
@@ -239,6 +262,7 @@ struct Tune {
     int chunk = 0;        // columns per pipeline pass
     int solve_ctas = 0;   // solver CTAs per SM
     int rb = 0;           // reduce: kept-system rows per TMA chunk
+    int fused = -1;       // fused kernel: index into FUSED_SHAPES (-1: the default shape)
 };
 
 struct Slot {
@@ -270,6 +294,7 @@ struct mgcm_rt_handle {
     bool quad = false;        // four-lane solvers for L <= 51 (mgcm_rt_config.solver)
     bool onchip = false;      // solvers with the per-system arrays on chip (mgcm_rt_config.solver)
     bool tmem = false;        // ... with tensor memory in front of shared memory
+    bool fused = false;       // one persistent fused kernel per call (mgcm_rt_config.solver)
     AeroConst aero{};         // aerosol optics constants (mgcm_rt_run_tracers)
     double *d_mie = nullptr;  // Mie tables on the device; null when the files were absent
     std::mutex mu;                                  // serialises the synchronous API
@@ -670,6 +695,42 @@ int launch_pipeline(mgcm_rt_handle *h, Slot &sl, cudaStream_t st, int total, int
     return MGCM_RT_OK;
 }
 
+// One persistent fused kernel over every column of the slot's segment table:
+// grid = the CTAs that fit the SMs at once, each with its own scratch; a tile
+// counter (cleared first) hands out the columns.  No chunking: the scratch
+// does not grow with the number of columns.
+int launch_fused(mgcm_rt_handle *h, Slot &sl, cudaStream_t st, int ncols, int max_nl, int &nk) {
+    const int si = sl.tune.fused >= 0 && sl.tune.fused < FUSED_NS ? sl.tune.fused : FUSED_DEFAULT;
+    const FusedShape sh = FUSED_SHAPES[si];
+    const bool mixed = h->cfg.precision == MGCM_RT_MIXED;
+    const FusedKernel kern = FUSED_KERNELS[mixed ? 1 : 0][si];
+    const size_t smem = fused_smem(sh.threads / 32, sh.tc);
+    int occ = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, sh.threads, smem) != cudaSuccess || occ < 1)
+        occ = 1;
+    const int grid = h->num_sms * occ;
+    size_t stride = 0;
+    pipe_bytes_per_col(max_nl, &stride);
+    const size_t cta = (fused_scratch_per_cta(sh.tc, max_nl, stride) + 255) / 256 * 256;
+    const int rc = arena_ensure(h, sl.pipe, cta * grid + 256, st);
+    if (rc) return rc;
+    unsigned char *scr = static_cast<unsigned char *>(sl.pipe.ptr);
+    unsigned int *ctr = reinterpret_cast<unsigned int *>(scr + cta * grid);
+    CK(cudaMemsetAsync(ctr, 0, sizeof(unsigned int), st));
+    kern<<<grid, sh.threads, smem, st>>>(sl.d_segs, ncols, max_nl, scr, cta, stride, h->d_kv, h->d_ki, h->d_kvf,
+                                         h->d_planck, h->K, ctr, sl.d_status, sl.d_nsys);
+    CK(cudaGetLastError());
+    nk += 1;
+    return MGCM_RT_OK;
+}
+
+// The radiation kernels of a call: the persistent fused kernel or the
+// multi-kernel pipeline, per the handle's form.
+int launch_body(mgcm_rt_handle *h, Slot &sl, cudaStream_t st, int total, int max_nl, int &nk, int max_chunk) {
+    return h->fused ? launch_fused(h, sl, st, total, max_nl, nk)
+                    : launch_pipeline(h, sl, st, total, max_nl, nk, max_chunk);
+}
+
 // Status words cleared, optional validation, kernels between ev0 and ev1.
 int launch_all(mgcm_rt_handle *h, Slot &sl, cudaStream_t st, int total, int max_nl, int max_chunk) {
     CK(cudaMemsetAsync(sl.d_status, 0, 256, st));
@@ -680,7 +741,7 @@ int launch_all(mgcm_rt_handle *h, Slot &sl, cudaStream_t st, int total, int max_
         ++nk;
     }
     CK(cudaEventRecord(sl.ev0, st));
-    const int rc = launch_pipeline(h, sl, st, total, max_nl, nk, max_chunk);
+    const int rc = launch_body(h, sl, st, total, max_nl, nk, max_chunk);
     if (rc) return rc;
     CK(cudaEventRecord(sl.ev1, st));
     sl.kernels = nk;
@@ -1441,7 +1502,8 @@ mgcm_rt_handle *mgcm_rt_create(const mgcm_rt_config *cfg, const char *data_dir, 
             return nullptr;
         }
     }
-    if (cfg->solver < MGCM_RT_SOLVER_AUTO || cfg->solver > MGCM_RT_SOLVER_TMEM) { *status = MGCM_RT_EINVAL; return nullptr; }
+    if (cfg->solver < MGCM_RT_SOLVER_AUTO || cfg->solver > MGCM_RT_SOLVER_FUSED) { *status = MGCM_RT_EINVAL; return nullptr; }
+    h->fused = cfg->solver == MGCM_RT_SOLVER_FUSED;
     h->tmem = cfg->solver == MGCM_RT_SOLVER_TMEM;
     h->quad = cfg->solver == MGCM_RT_SOLVER_QUAD;
     h->onchip = cfg->solver == MGCM_RT_SOLVER_ONCHIP;
@@ -1826,7 +1888,7 @@ int time_shape(mgcm_rt_graph *g, const Tune &t, int cols, float &ms) {
     for (int rep = 0; rep < 2; ++rep) {
         CK(cudaMemsetAsync(sl.d_status, 0, 256, st));
         CK(cudaEventRecord(sl.ev0, st));
-        int rc = launch_pipeline(h, sl, st, cols, g->max_nl, nk, g->max_chunk);
+        int rc = launch_body(h, sl, st, cols, g->max_nl, nk, g->max_chunk);
         if (rc) return rc;
         CK(cudaEventRecord(sl.ev1, st));
         CK(cudaStreamSynchronize(st));
@@ -1906,7 +1968,20 @@ int mgcm_rt_graph_create(mgcm_rt_handle *h, int nbatch, const mgcm_rt_batch_in *
     if (rc) return fail(rc);
     float t_best = t_def;
     int ncand = 1;
-    if (autotune) {
+    if (autotune && h->fused) {   // fused kernel: columns per tile, threads per CTA, CTAs per SM
+        for (int q = 0; q < FUSED_NS; ++q) {
+            if (q == FUSED_DEFAULT) continue;
+            Tune t = best;
+            t.fused = q;
+            float ms = 0.f;
+            if ((rc = time_shape(g, t, sample, ms))) return fail(rc);
+            ++ncand;
+            if (ms < t_best) {
+                t_best = ms;
+                best = t;
+            }
+        }
+    } else if (autotune) {
         auto consider = [&](Tune t) -> int {
             float ms = 0.f;
             const int r = time_shape(g, t, sample, ms);
@@ -1948,7 +2023,7 @@ int mgcm_rt_graph_create(mgcm_rt_handle *h, int nbatch, const mgcm_rt_batch_in *
     if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return fail(MGCM_RT_ECUDA);
     int crc = MGCM_RT_OK;
     if (cudaMemsetAsync(sl.d_status, 0, 256, st) != cudaSuccess) crc = MGCM_RT_ECUDA;
-    if (!crc) crc = launch_pipeline(h, sl, st, total, max_nl, nk, g->max_chunk);
+    if (!crc) crc = launch_body(h, sl, st, total, max_nl, nk, g->max_chunk);
     if (!crc) crc = post_status(sl, st);
     cudaGraph_t gr = nullptr;
     const cudaError_t ce = cudaStreamEndCapture(st, &gr);
@@ -1968,6 +2043,13 @@ int mgcm_rt_graph_create(mgcm_rt_handle *h, int nbatch, const mgcm_rt_batch_in *
     inf.best_ms = t_best;
     inf.kernels = nk;
     inf.columns = total;
+    if (h->fused) {
+        const FusedShape fs = FUSED_SHAPES[best.fused >= 0 ? best.fused : FUSED_DEFAULT];
+        inf.chunk_cols = fs.tc;
+        inf.solve_ctas_per_sm = fs.minb;
+        inf.reduce_rows = 0;
+        inf.threads_per_cta = fs.threads;
+    }
     *graph = g;
     return MGCM_RT_OK;
 }

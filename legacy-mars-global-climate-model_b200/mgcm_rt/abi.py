@@ -39,7 +39,7 @@ class RequestInfo(C.Structure):
                 ("device_end_ms", C.c_double)]
 
 
-SOLVER_AUTO, SOLVER_THREAD, SOLVER_QUAD, SOLVER_ONCHIP, SOLVER_TMEM = 0, 1, 2, 3, 4
+SOLVER_AUTO, SOLVER_THREAD, SOLVER_QUAD, SOLVER_ONCHIP, SOLVER_TMEM, SOLVER_FUSED = 0, 1, 2, 3, 4, 5
 
 
 _IN_PTRS = ("sigma", "sol", "plev", "tlev", "pmid", "tmid", "qh2o", "tauref", "qextrefdst",
@@ -97,7 +97,8 @@ class BatchState(C.Structure):
 class Tune(C.Structure):
     _fields_ = [("chunk_cols", C.c_int), ("solve_ctas_per_sm", C.c_int), ("reduce_rows", C.c_int),
                 ("candidates", C.c_int), ("tuning_cols", C.c_int), ("default_ms", C.c_double),
-                ("best_ms", C.c_double), ("kernels", C.c_int), ("columns", C.c_int)]
+                ("best_ms", C.c_double), ("kernels", C.c_int), ("columns", C.c_int),
+                ("threads_per_cta", C.c_int)]
 
 
 _lib = None

@@ -66,3 +66,58 @@ def test_graph_rejects_host_batches(data_dir):
         assert rc == -1 and not g.value
     finally:
         rt.close()
+
+
+@pytest.mark.parametrize("precision", [abi.FP64, abi.MIXED])
+def test_graph_fused_persistent_kernel(data_dir, otables, precision):
+    """The persistent fused form captured as a graph: one kernel launch per
+    replay over members of three layer counts, autotuned over its launch
+    shapes; FP64 matches the oracle to 1e-12, MIXED stays within 1e-3 on
+    fluxes and 1e-2 K/sol on heating."""
+    import torch
+    from helpers import mixed_errors
+    rt = abi.Radiation(data_dir, max_layers=48, precision=precision, validate=False, solver=abi.SOLVER_FUSED)
+    try:
+        specs = [(400, 24, 91), (250, 36, 92), (180, 48, 93), (1, 36, 94), (333, 24, 95)]
+        host = [synth.make_batch(n, L=L, seed=s, cloud=True) for n, L, s in specs]
+        dev = [_device(b) for b in host]
+        g = rt.graph(dev, autotune=True)
+        try:
+            info = g.info()
+            assert info["kernels"] == 1, info
+            assert info["candidates"] >= 2 and info["threads_per_cta"] in (128, 256), info
+            for _ in range(2):
+                g.launch()
+                torch.cuda.synchronize()
+                assert g.status() == 0
+            for b, o in zip(host, g.outs):
+                ref = oracle.run_batch(otables, b)
+                got = to_numpy(o)
+                if precision == abi.FP64:
+                    err = compare(b, got, ref, 1e-12)
+                    assert max(err.values()) <= 1e-12, err
+                else:
+                    e = mixed_errors(b, got, ref)
+                    assert e["flux_max"] <= 1e-3 and e["heat_dT_Ksol_max"] <= 1e-2, e
+        finally:
+            g.close()
+    finally:
+        rt.close()
+
+
+def test_fused_uneven_multi_grid_and_host_calls(data_dir, otables):
+    """The fused form through run_multi (uneven grids in one launch) and the
+    host-buffer call, FP64 against the oracle."""
+    rt = abi.Radiation(data_dir, max_layers=99, precision=abi.FP64, validate=True, solver=abi.SOLVER_FUSED)
+    try:
+        bs = [synth.make_batch(70, L=24, seed=96, cloud=True), synth.make_batch(33, L=99, seed=97, cloud=True),
+              synth.make_batch(41, L=2, seed=98, cloud=False)]
+        outs = rt.run_multi([_device(b) for b in bs])
+        for b, o in zip(bs, outs):
+            err = compare(b, to_numpy(o), oracle.run_batch(otables, b), 1e-12)
+            assert max(err.values()) <= 1e-12, err
+        b = synth.make_batch(9000, L=24, seed=99, cloud=True)
+        err = compare(b, to_numpy(rt.run(b)), oracle.run_batch(otables, b), 1e-12)
+        assert max(err.values()) <= 1e-12, err
+    finally:
+        rt.close()

@@ -123,12 +123,12 @@ def test_input_errors_are_status_codes(rt):
 def test_four_lane_and_thread_solvers_match_oracle(data_dir, otables, L):
     """Every solver form (one thread per system with its arrays in local
     memory; four lanes per system for L <= 51; one thread per system with its
-    arrays on chip, in shared memory or in tensor memory and shared memory)
-    reproduces the oracle at 1e-12, at layer counts that split unevenly over
-    the four lanes."""
+    arrays on chip, in shared memory or in tensor memory and shared memory;
+    the persistent fused kernel) reproduces the oracle at 1e-12, at layer
+    counts that split unevenly over the four lanes."""
     b = synth.make_batch(48, L=L, seed=900 + L, cloud=True)
     ref = oracle.run_batch(otables, b)
-    for solver in (abi.SOLVER_THREAD, abi.SOLVER_QUAD, abi.SOLVER_ONCHIP, abi.SOLVER_TMEM):
+    for solver in (abi.SOLVER_THREAD, abi.SOLVER_QUAD, abi.SOLVER_ONCHIP, abi.SOLVER_TMEM, abi.SOLVER_FUSED):
         rt = abi.Radiation(data_dir, max_layers=max(L, 1), precision=abi.FP64, validate=True, solver=solver)
         try:
             err = compare(b, to_numpy(rt.run(b)), ref, RTOL)
