@@ -29,6 +29,11 @@
  *   NLAY = L+1 (L_NLAYRAD)        layer outputs    [ncol][NLAY]
  *   DETAU, CUMTAUV                [ncol][17][7]    (Fortran A(nw,ng,col))
  *
+ * Device pointers: a call is ordered after all work already queued on the
+ * legacy default stream (cudaMemcpy, a framework's default-stream kernels),
+ * or, after mgcm_rt_set_stream, on the caller's stream; device buffers
+ * written on any other stream must be complete before the call.
+ *
  * Errors are negative return codes (never abort/exit; the reference STOPs,
  * code/gfluxi.f90:65).  A handle is thread-safe: calls on one handle are
  * serialised by an internal lock and run on the handle's own CUDA stream.

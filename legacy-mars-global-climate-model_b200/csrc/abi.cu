@@ -270,6 +270,7 @@ struct Slot {
     cudaStream_t aux = nullptr;   // the visible solve runs here, beside the IR solve
     cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, done = nullptr;
+    cudaEvent_t after_legacy = nullptr;   // orders the slot after the legacy default stream
     SegTable *h_segs = nullptr, *d_segs = nullptr;
     uint32_t *d_status = nullptr, *h_status = nullptr;
     unsigned long long *d_nsys = nullptr, *h_nsys = nullptr;
@@ -455,6 +456,16 @@ cudaStream_t sync_stream(mgcm_rt_handle *h) {
     return h->user_stream ? h->user_stream : h->slots[0]->stream;
 }
 
+// Device-pointer calls: the slots' streams are non-blocking, so they do not
+// wait for work the caller queued on the legacy default stream (cudaMemcpy,
+// a framework's default-stream fills of the very buffers passed in).  An
+// event recorded there and waited on first orders the call after all of it.
+int after_legacy_stream(Slot &sl, cudaStream_t st) {
+    CK(cudaEventRecord(sl.after_legacy, cudaStreamLegacy));
+    CK(cudaStreamWaitEvent(st, sl.after_legacy, 0));
+    return MGCM_RT_OK;
+}
+
 // Grows an arena within the handle's HBM budget (arenas never shrink).
 int arena_ensure(mgcm_rt_handle *h, Arena &a, size_t bytes, cudaStream_t s) {
     if (a.bytes >= bytes) return MGCM_RT_OK;
@@ -481,6 +492,7 @@ int slot_init(Slot &s) {
     CK(cudaEventCreate(&s.ev0));
     CK(cudaEventCreate(&s.ev1));
     CK(cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&s.after_legacy, cudaEventDisableTiming));
     CK(cudaMallocHost(&s.h_segs, sizeof(SegTable)));
     CK(cudaMalloc(&s.d_segs, sizeof(SegTable)));
     CK(cudaMalloc(&s.d_status, 256));
@@ -508,6 +520,7 @@ void slot_free(mgcm_rt_handle *h, Slot &s) {
     if (s.ev0) cudaEventDestroy(s.ev0);
     if (s.ev1) cudaEventDestroy(s.ev1);
     if (s.done) cudaEventDestroy(s.done);
+    if (s.after_legacy) cudaEventDestroy(s.after_legacy);
     if (s.aux) cudaStreamSynchronize(s.aux);
     if (s.fork_ev) cudaEventDestroy(s.fork_ev);
     if (s.join_ev) cudaEventDestroy(s.join_ev);
@@ -776,6 +789,7 @@ int issue_job(mgcm_rt_handle *h, Slot &sl, cudaStream_t st, const mgcm_rt_batch_
     sd.ptrop = in.ptrop;
     std::vector<ArrSpec> arrs;
     if (in.device_ptrs) {
+        if (const int rc = after_legacy_stream(sl, st)) return rc;
         fill_direct(sd, in, out);
         // shift every per-column pointer to the job's first column
         arrs = arrays_of(in, out, z, sd);
@@ -850,6 +864,9 @@ int run_device(mgcm_rt_handle *h, int nbatch, const mgcm_rt_batch_in *in, mgcm_r
     }
     if (total == 0) return MGCM_RT_OK;
     tab.total_cols = total;
+    if (!h->user_stream) {
+        if (const int rc = after_legacy_stream(sl, st)) return rc;
+    }
     CK(cudaMemcpyAsync(sl.d_segs, sl.h_segs, sizeof(SegTable), cudaMemcpyHostToDevice, st));
     // pipeline chunk: bounded by a quarter of the budget
     const size_t per_col = pipe_bytes_per_col(max_nl);
@@ -916,6 +933,9 @@ std::vector<int> job_ends(int n, int max_job, int first) {
 // synchronous slots, forked from and joined back into the caller's stream.
 int run_host(mgcm_rt_handle *h, int nbatch, const mgcm_rt_batch_in *in, mgcm_rt_batch_out *out) {
     cudaStream_t ust = sync_stream(h);
+    if (!h->user_stream) {
+        if (const int rc = after_legacy_stream(*h->slots[0], ust)) return rc;
+    }
     CK(cudaEventRecord(h->fork, ust));
     for (auto &s : h->slots) CK(cudaStreamWaitEvent(s->stream, h->fork, 0));
     uint32_t acc = 0;
@@ -1263,6 +1283,9 @@ int issue_tracer_job(mgcm_rt_handle *h, Slot &sl, cudaStream_t st, const mgcm_rt
 int run_tracers(mgcm_rt_handle *h, const mgcm_rt_batch_tracers &in, mgcm_rt_batch_out &out,
                 const mgcm_rt_batch_state *stt = nullptr) {
     cudaStream_t ust = sync_stream(h);
+    if (!h->user_stream) {
+        if (const int rc = after_legacy_stream(*h->slots[0], ust)) return rc;
+    }
     CK(cudaEventRecord(h->fork, ust));
     for (auto &s : h->slots) CK(cudaStreamWaitEvent(s->stream, h->fork, 0));
     uint32_t acc = 0;
@@ -1677,6 +1700,9 @@ int mgcm_rt_dsolflux(mgcm_rt_handle *h, int ncol, int device_ptrs, const double 
     if (rc) return rc;
     Slot &sl = *h->slots[0];
     cudaStream_t st = sync_stream(h);
+    if (device_ptrs && !h->user_stream) {
+        if (const int rc = after_legacy_stream(*h->slots[0], st)) return rc;
+    }
     const double *ds = sol, *da = acosz, *dd = detau, *dn = dndiffv;
     double *dout = dnvflux;
     if (!device_ptrs) {
@@ -1716,6 +1742,9 @@ int mgcm_rt_debug_bins(mgcm_rt_handle *h, const mgcm_rt_batch_in *in, int *mt, i
     if (int rc = finish_pending(h)) return rc;
     Slot &sl = *h->slots[0];
     cudaStream_t st = sync_stream(h);
+    if (!h->user_stream) {
+        if (const int rc0 = after_legacy_stream(sl, st)) return rc0;
+    }
     const Sizes z = sizes_of(*in);
     SegDev sd{};
     sd.ncol = (int)z.ncol;
@@ -2122,6 +2151,9 @@ extern "C" int mgcm_rt_run_noalloc(mgcm_rt_handle *h, const mgcm_rt_batch_in *in
     if (rc) return rc;
     Slot &sl = *h->slots[0];
     cudaStream_t stream = sync_stream(h);
+    if (!h->user_stream) {
+        if (const int rc2 = after_legacy_stream(sl, stream)) return rc2;
+    }
     unsigned char *scr = nullptr;
     rc = noalloc_scratch(h->device, &scr);
     if (rc) return rc;
