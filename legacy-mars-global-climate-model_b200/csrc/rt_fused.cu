@@ -31,8 +31,10 @@ namespace mgcm {
 using namespace fp64;
 
 // Per-warp reduce scratch: the folded FZERO of 7 + 5 bands, FMNET of both
-// families per level, the top-of-atmosphere values.
-constexpr int FZ_WARP_DOUBLES = 12 + 2 * (D_MAXNL + 2) + 4;
+// families per level, the top-of-atmosphere values, and one family's kept
+// rows in order (three weights and a scratch row index each).
+constexpr int FZ_WARP_DOUBLES = 12 + 2 * (D_MAXNL + 2) + 4 + 3 * NSYS_V + (NSYS_V + 1) / 2;
+constexpr int FZ_RB = 4;   // rows whose loads are issued before they are summed
 constexpr int FZ_LPL = (D_MAXNL + 31) / 32;   // levels per lane
 
 // Shared memory of a CTA of `warps` warps and TC columns per tile.
@@ -164,9 +166,14 @@ rt_fused(const SegTable *__restrict__ st, int ncols, int max_nl, unsigned char *
         // ((v*DWNI)*GWEIGHT)*(1-FZEROI), Gauss point 17 (v*DWNI)*FZERO, where
         // FZERO has the weights of the TLIMIT-skipped points folded in, in
         // ascending order (code/sfluxv.f90:72-75,102-162,
-        // code/sfluxi.f90:72-75,95-143).
+        // code/sfluxi.f90:72-75,95-143).  Per family the lanes first lay out
+        // the kept rows' positions and weights in order; then each level's
+        // sums run over the rows in that order, FZ_RB rows' loads issued
+        // before they are added.
         double *fzf = rbase + (size_t)warp * FZ_WARP_DOUBLES;
         double *fmv = fzf + 12, *fmi = fmv + (D_MAXNL + 2), *misc = fmi + (D_MAXNL + 2);
+        double *wa = misc + 4, *wb = wa + NSYS_V, *we = wb + NSYS_V;
+        int *rpos = reinterpret_cast<int *>(we + NSYS_V);
         for (int j = warp; j < ng; j += WARPS) {
             const int g = g0 + j;
             const SegDev &sg = st->seg[find_seg(st, g)];
@@ -188,17 +195,14 @@ rt_fused(const SegTable *__restrict__ st, int ncols, int max_nl, unsigned char *
             __syncwarp();
             for (int fam = 0; fam < 2; ++fam) {
                 const bool vis = fam == 0;
-                double acc[3][FZ_LPL], top = 0.0, dif = 0.0;
-#pragma unroll
-                for (int q = 0; q < 3; ++q)
-#pragma unroll
-                    for (int r = 0; r < FZ_LPL; ++r) acc[q][r] = 0.0;
+                // kept rows of the family in order: scratch row index and weights
+                int nrow = 0;
                 if (!vis || day) {
                     const int w0 = vis ? 0 : SCREEN_GROUPS_V, w1 = vis ? SCREEN_GROUPS_V : SCREEN_GROUPS;
                     for (int gw = w0; gw < w1; ++gw) {
                         const int gb = s.meta[2 * gw], gn = s.meta[2 * gw + 1];
-                        for (int k = 0; k < gn; ++k) {
-                            const int li = gb + k;
+                        if (lane < gn) {
+                            const int li = gb + lane;
                             const int sidx = list[vis ? li : TC * NSYS - 1 - li] & 255;
                             const int q = vis ? sidx : sidx - NSYS_V;
                             const int nw = q / D_NG + 1, ngs = q % D_NG + 1;
@@ -212,48 +216,72 @@ rt_fused(const SegTable *__restrict__ st, int ncols, int max_nl, unsigned char *
                                 if (ngs < D_NG) { b = K.gweight[ngs - 1]; e = 1.0 - K.fzeroi[nw - 1]; }
                                 else { b = fzf[D_NV + nw - 1]; e = 1.0; }
                             }
-                            auto wt = [&](double v) { return ((v * a) * b) * e; };
-                            const size_t rr = vis ? (size_t)li : (size_t)TC * NSYS_V + li;
-                            const double *pr = fl + rr * row;
+                            wa[nrow + lane] = a;
+                            wb[nrow + lane] = b;
+                            we[nrow + lane] = e;
+                            rpos[nrow + lane] = vis ? li : TC * NSYS_V + li;
+                        }
+                        nrow += gn;
+                    }
+                }
+                __syncwarp();
+                double top = 0.0, dif = 0.0;
+                for (int r = 0; r < FZ_LPL && 32 * r < NL; ++r) {
+                    const int l = lane + 1 + 32 * r;
+                    const bool lv = l <= NL;
+                    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+                    for (int f0 = 0; f0 < nrow; f0 += FZ_RB) {
+                        double up[FZ_RB], dn[FZ_RB], t0[FZ_RB], t1[FZ_RB];
 #pragma unroll
-                            for (int r = 0; r < FZ_LPL; ++r) {
-                                const int l = lane + 1 + 32 * r;
-                                if (l > NL) break;
-                                const double up = pr[l - 1], dn = pr[max_nl + l - 1];
-                                acc[0][r] = acc[0][r] + wt(up - dn);
-                                acc[1][r] = acc[1][r] + wt(up);
-                                acc[2][r] = acc[2][r] + wt(dn);
+                        for (int q = 0; q < FZ_RB; ++q) {
+                            up[q] = dn[q] = t0[q] = t1[q] = 0.0;
+                            if (f0 + q < nrow) {
+                                const size_t rr = (size_t)rpos[f0 + q];
+                                const double *pr = fl + rr * row;
+                                if (lv) {
+                                    up[q] = pr[l - 1];
+                                    dn[q] = pr[max_nl + l - 1];
+                                }
+                                if (r == 0) {
+                                    const double *skp = sc + rr * 4;
+                                    t0[q] = vis ? skp[0] - skp[1] : skp[0];
+                                    t1[q] = skp[2];
+                                }
                             }
-                            const double *sk = sc + rr * 4;
-                            if (vis) {
-                                top = top + wt(sk[0] - sk[1]);
-                                dif = dif + wt(sk[2]);
-                            } else {
-                                top = top + wt(sk[0]);
+                        }
+#pragma unroll
+                        for (int q = 0; q < FZ_RB; ++q) {
+                            if (f0 + q < nrow) {
+                                const double a = wa[f0 + q], b = wb[f0 + q], e = we[f0 + q];
+                                auto wt = [&](double v) { return ((v * a) * b) * e; };
+                                a0 = a0 + wt(up[q] - dn[q]);
+                                a1 = a1 + wt(up[q]);
+                                a2 = a2 + wt(dn[q]);
+                                if (r == 0) {
+                                    top = top + wt(t0[q]);
+                                    if (vis) dif = dif + wt(t1[q]);
+                                }
                             }
                         }
                     }
-                }
-#pragma unroll
-                for (int r = 0; r < FZ_LPL; ++r) {
-                    const int l = lane + 1 + 32 * r;
-                    if (l > NL) break;
-                    const size_t o = (size_t)c * NL + l - 1;
-                    if (vis) {
-                        sg.fmnetv[o] = acc[0][r];
-                        sg.fluxupv[o] = acc[1][r];
-                        sg.fluxdnv[o] = acc[2][r];
-                        fmv[l] = acc[0][r];
-                        if (l == NL) {
-                            sg.dnvflux[c] = acc[2][r];
-                            sg.fluxsurf[c] = (1.0 - sg.als[c]) * acc[2][r];
+                    if (lv) {
+                        const size_t o = (size_t)c * NL + l - 1;
+                        if (vis) {
+                            sg.fmnetv[o] = a0;
+                            sg.fluxupv[o] = a1;
+                            sg.fluxdnv[o] = a2;
+                            fmv[l] = a0;
+                            if (l == NL) {
+                                sg.dnvflux[c] = a2;
+                                sg.fluxsurf[c] = (1.0 - sg.als[c]) * a2;
+                            }
+                        } else {
+                            sg.fmneti[o] = a0;
+                            sg.fluxupi[o] = a1;
+                            sg.fluxdni[o] = a2;
+                            fmi[l] = a0;
+                            if (l == NL) sg.dnirflux[c] = a2;
                         }
-                    } else {
-                        sg.fmneti[o] = acc[0][r];
-                        sg.fluxupi[o] = acc[1][r];
-                        sg.fluxdni[o] = acc[2][r];
-                        fmi[l] = acc[0][r];
-                        if (l == NL) sg.dnirflux[c] = acc[2][r];
                     }
                 }
                 if (lane == 0) {
@@ -267,6 +295,7 @@ rt_fused(const SegTable *__restrict__ st, int ncols, int max_nl, unsigned char *
                         misc[1] = top;
                     }
                 }
+                __syncwarp();   // the row tables are rebuilt for the next family
             }
             __syncwarp();
             const double *plev = sg.plev + (size_t)c * LEV;
@@ -308,6 +337,8 @@ FUSED_INST(8, 128, 8)
 FUSED_INST(4, 128, 6)
 FUSED_INST(4, 256, 4)
 FUSED_INST(8, 256, 4)
+FUSED_INST(16, 256, 4)
+FUSED_INST(8, 512, 2)
 #undef FUSED_INST
 #undef FUSED_ARGS
 
