@@ -30,6 +30,7 @@
 #include "rt_prep.cuh"
 #include "rt_column.cuh"
 #include "tables.h"
+#include <nvtx3/nvToolsExt.h>
 
 namespace mgcm {
 __global__ void rt_fp64_kernel(const SegTable *__restrict__ st, const double *__restrict__ kv,
@@ -112,6 +113,16 @@ __global__ void rt_bins_decode(const SegTable *__restrict__ st, int ncol, int ma
 using namespace mgcm;
 
 namespace {
+
+// NVTX range for the duration of a scope: each entry point, each job a slot
+// issues and each graph replay shows up by name in a timeline profiler
+// (header-only NVTX 3; a no-op when no tool is attached).
+struct NvtxRange {
+    explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange &) = delete;
+    NvtxRange &operator=(const NvtxRange &) = delete;
+};
 
 constexpr int BLOCK = 224;
 
@@ -545,6 +556,10 @@ int configure_kernels(int device) {
         for (int q = 0; q < OC_NT; ++q)
             CK(cudaFuncSetAttribute((const void *)OC_KERNELS[f][q], cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)SMEM_CAP));
+    for (int f = 0; f < 2; ++f)
+        for (int q = 0; q < FUSED_NS; ++q)
+            CK(cudaFuncSetAttribute((const void *)FUSED_KERNELS[f][q], cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)(SMEM_CAP - 1024)));
     for (int f = 0; f < 3; ++f)
         for (int q = 0; q < TM_NW; ++q)
             CK(cudaFuncSetAttribute((const void *)TM_KERNELS[f][q], cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -781,6 +796,7 @@ int post_status(Slot &sl, cudaStream_t st) {
 // batch in/out), the kernels and the copies back; records sl.done.
 int issue_job(mgcm_rt_handle *h, Slot &sl, cudaStream_t st, const mgcm_rt_batch_in &in,
               const mgcm_rt_batch_out &out, int c0, int c1) {
+    NvtxRange nvtx_range("mgcm_rt job");
     const Sizes z = sizes_of(in);
     const size_t n = (size_t)(c1 - c0);
     SegDev sd{};
@@ -1070,6 +1086,7 @@ int check_state(const mgcm_rt_handle *h, const mgcm_rt_batch_state *in, const mg
 int issue_tracer_job(mgcm_rt_handle *h, Slot &sl, cudaStream_t st, const mgcm_rt_batch_tracers &in,
                      const mgcm_rt_batch_out &out, int c0, int c1,
                      const mgcm_rt_batch_state *stt = nullptr) {
+    NvtxRange nvtx_range("mgcm_rt tracer job");
     const size_t n = (size_t)(c1 - c0);
     const int L = in.nlayers, lev = 2 * L + 3, lev1 = lev + 1, nl = L + 1;
     SegDev sd{};
@@ -1638,6 +1655,7 @@ void mgcm_rt_destroy(mgcm_rt_handle *h) {
 }
 
 int mgcm_rt_run(mgcm_rt_handle *h, const mgcm_rt_batch_in *in, mgcm_rt_batch_out *out) {
+    NvtxRange nvtx_range("mgcm_rt_run");
     if (!h || !in || !out) return MGCM_RT_EINVAL;
     std::lock_guard<std::mutex> lk(h->mu);
     if (cudaSetDevice(h->device) != cudaSuccess) return MGCM_RT_ECUDA;
@@ -1646,6 +1664,7 @@ int mgcm_rt_run(mgcm_rt_handle *h, const mgcm_rt_batch_in *in, mgcm_rt_batch_out
 
 int mgcm_rt_run_multi(mgcm_rt_handle *h, int nbatch, const mgcm_rt_batch_in *in,
                       mgcm_rt_batch_out *out) {
+    NvtxRange nvtx_range("mgcm_rt_run_multi");
     if (!h || !in || !out) return MGCM_RT_EINVAL;
     std::lock_guard<std::mutex> lk(h->mu);
     if (cudaSetDevice(h->device) != cudaSuccess) return MGCM_RT_ECUDA;
@@ -1653,6 +1672,7 @@ int mgcm_rt_run_multi(mgcm_rt_handle *h, int nbatch, const mgcm_rt_batch_in *in,
 }
 
 int mgcm_rt_enqueue(mgcm_rt_handle *h, const mgcm_rt_batch_in *in, mgcm_rt_batch_out *out) {
+    NvtxRange nvtx_range("mgcm_rt_enqueue");
     if (!h || !in || !out) return MGCM_RT_EINVAL;
     std::lock_guard<std::mutex> lk(h->mu);
     if (cudaSetDevice(h->device) != cudaSuccess) return MGCM_RT_ECUDA;
@@ -1785,6 +1805,7 @@ int mgcm_rt_debug_bins(mgcm_rt_handle *h, const mgcm_rt_batch_in *in, int *mt, i
 }
 
 int mgcm_rt_run_state(mgcm_rt_handle *h, const mgcm_rt_batch_state *in, mgcm_rt_batch_out *out) {
+    NvtxRange nvtx_range("mgcm_rt_run_state");
     const int rc = check_state(h, in, out);
     if (rc || in->ncol == 0) return rc;
     std::lock_guard<std::mutex> lk(h->mu);
@@ -1796,6 +1817,7 @@ int mgcm_rt_run_state(mgcm_rt_handle *h, const mgcm_rt_batch_state *in, mgcm_rt_
 }
 
 int mgcm_rt_run_tracers(mgcm_rt_handle *h, const mgcm_rt_batch_tracers *in, mgcm_rt_batch_out *out) {
+    NvtxRange nvtx_range("mgcm_rt_run_tracers");
     const int rc = check_tracers(h, in, out);
     if (rc || in->ncol == 0) return rc;
     std::lock_guard<std::mutex> lk(h->mu);
@@ -2085,6 +2107,7 @@ int mgcm_rt_graph_create(mgcm_rt_handle *h, int nbatch, const mgcm_rt_batch_in *
 }
 
 int mgcm_rt_graph_launch(mgcm_rt_graph *g, void *stream) {
+    NvtxRange nvtx_range("mgcm_rt_graph_launch");
     if (!g || !g->exec) return MGCM_RT_EINVAL;
     cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : g->slot.stream;
     CK(cudaGraphLaunch(g->exec, st));
@@ -2141,6 +2164,7 @@ int noalloc_scratch(int device, unsigned char **ptr) {
 
 extern "C" int mgcm_rt_run_noalloc(mgcm_rt_handle *h, const mgcm_rt_batch_in *in,
                                    mgcm_rt_batch_out *out) {
+    NvtxRange nvtx_range("mgcm_rt_run_noalloc");
     if (!h || !in || !out) return MGCM_RT_EINVAL;
     if (!in->device_ptrs) return MGCM_RT_EINVAL;   // host buffers would need staging memory
     std::lock_guard<std::mutex> lk(h->mu);
