@@ -2012,7 +2012,10 @@ int mgcm_rt_graph_create(mgcm_rt_handle *h, int nbatch, const mgcm_rt_batch_in *
     // autotune: coordinate descent over chunk, solver CTAs per SM and reduce
     // rows per chunk, each shape timed (best of two) on the first columns
     Tune best{};
-    const int sample = std::min(total, 131072);
+    // tuning sample: the first 131,072 columns for the pipeline; the whole
+    // batch (up to 1M columns) for the fused kernel, whose best shape depends
+    // on the mix of layer counts, which the first members need not represent
+    const int sample = h->fused ? std::min(total, 1 << 20) : std::min(total, 131072);
     float t_def = 0.f;
     int rc = time_shape(g, best, sample, t_def);
     if (rc) return fail(rc);
