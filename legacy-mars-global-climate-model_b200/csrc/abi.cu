@@ -145,15 +145,17 @@ using FusedKernel = void (*)(const SegTable *__restrict__, int, int, unsigned ch
                              const double *__restrict__, const RtConst, unsigned int *, uint32_t *,
                              unsigned long long *);
 struct FusedShape { int tc, threads, minb; };
-constexpr int FUSED_NS = 10;
+constexpr int FUSED_NS = 13;
 constexpr FusedShape FUSED_SHAPES[FUSED_NS] = {{2, 128, 8}, {4, 128, 8}, {8, 128, 8}, {4, 128, 6},
                                                {4, 256, 4}, {8, 256, 4}, {16, 256, 4}, {8, 512, 2},
-                                               {8, 256, 3}, {16, 384, 2}};
-constexpr int FUSED_DEFAULT = 5;
+                                               {8, 256, 3}, {16, 384, 2}, {16, 256, 3}, {24, 384, 2},
+                                               {16, 320, 2}};
+constexpr int FUSED_DEFAULT = 9;   // the tuner's choice for the 889,920-column ensemble
 #define FZ_ROW(F) {rt_fused<F, 2, 128, 8>, rt_fused<F, 4, 128, 8>, rt_fused<F, 8, 128, 8>,  \
                    rt_fused<F, 4, 128, 6>, rt_fused<F, 4, 256, 4>, rt_fused<F, 8, 256, 4>,  \
                    rt_fused<F, 16, 256, 4>, rt_fused<F, 8, 512, 2>, rt_fused<F, 8, 256, 3>,   \
-                   rt_fused<F, 16, 384, 2>}
+                   rt_fused<F, 16, 384, 2>, rt_fused<F, 16, 256, 3>, rt_fused<F, 24, 384, 2>, \
+                   rt_fused<F, 16, 320, 2>}
 const FusedKernel FUSED_KERNELS[2][FUSED_NS] = {FZ_ROW(false), FZ_ROW(true)};
 #undef FZ_ROW
 

@@ -426,6 +426,9 @@ FUSED_INST(16, 256, 4)
 FUSED_INST(8, 512, 2)
 FUSED_INST(8, 256, 3)
 FUSED_INST(16, 384, 2)
+FUSED_INST(16, 256, 3)
+FUSED_INST(24, 384, 2)
+FUSED_INST(16, 320, 2)
 #undef FUSED_INST
 #undef FUSED_ARGS
 
