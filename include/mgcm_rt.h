@@ -309,6 +309,14 @@ int mgcm_rt_dsolflux(mgcm_rt_handle *h, int ncol, int device_ptrs, const double 
 int mgcm_rt_debug_bins(mgcm_rt_handle *h, const mgcm_rt_batch_in *in, int *mt, int *mp, int *nh2o,
                        int *nplanck, double *wratio, double *lcoef);
 
+/* Self-check of the device waits (no counterpart in the reference): runs a
+ * kernel whose wait can never be satisfied -- an mbarrier armed for bytes no
+ * copy delivers -- through the same bounded wait the kernels use, and
+ * returns MGCM_RT_OK when that wait gave up (about a second, *seconds if not
+ * NULL) and reported it in the status word, MGCM_RT_ECUDA otherwise.  No
+ * fault and no hang: the kernel returns normally and the handle stays usable. */
+int mgcm_rt_check_wait_bound(mgcm_rt_handle *h, double *seconds);
+
 int mgcm_rt_get_stats(mgcm_rt_handle *h, mgcm_rt_stats *st);
 
 /* Host copies of the set-up tables, laid out as the reference modules hold
