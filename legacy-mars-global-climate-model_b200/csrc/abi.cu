@@ -1827,7 +1827,12 @@ int mgcm_rt_check_wait_bound(mgcm_rt_handle *h, double *seconds) {
     float ms = 0.f;
     cudaEventElapsedTime(&ms, sl.ev0, sl.ev1);
     if (seconds) *seconds = ms * 1e-3;
-    return (*sl.h_status & ST_TMA_TIMEOUT) ? MGCM_RT_OK : MGCM_RT_ECUDA;
+    const bool gave_up = (*sl.h_status & ST_TMA_TIMEOUT) != 0;
+    // leave the slot's status clean for the next call
+    CK(cudaMemsetAsync(sl.d_status, 0, 256, st));
+    CK(cudaStreamSynchronize(st));
+    *sl.h_status = 0;
+    return gave_up ? MGCM_RT_OK : MGCM_RT_ECUDA;
 }
 
 int mgcm_rt_run_state(mgcm_rt_handle *h, const mgcm_rt_batch_state *in, mgcm_rt_batch_out *out) {

@@ -50,10 +50,22 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
     return ok != 0;
 }
 
-// Bounded wait for the phase with the given parity: about a second at most.
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Bounded wait for the phase with the given parity: gives up after one
+// second of the global timer (each try_wait may itself block for a
+// hardware-defined interval, so an iteration count alone does not bound the
+// time), or after 2^22 tries should the timer not advance.
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32_t *status) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = global_ns();
     for (uint32_t it = 0; it < (1u << 22); ++it) {
         if (mbar_try_wait(bar, parity)) return true;
+        if (global_ns() - t0 > 1000000000ull) break;
         if (it > 64) __nanosleep(256);
     }
     atomicOr(status, ST_TMA_TIMEOUT);
