@@ -183,8 +183,11 @@ template __global__ void rt_fp64_screen<true>(SCREEN_ARGS);
 #undef SCREEN_ARGS
 
 // K2: solve the listed systems of one family, one thread per system.
+#ifndef MGCM_IR_SOLVE_MINB
+#define MGCM_IR_SOLVE_MINB 8   // resident CTAs per SM asked of the IR solve
+#endif
 template <bool VIS>
-__global__ void __launch_bounds__(128, VIS ? 6 : 8)   // 80 / 64 registers: measured best occupancy
+__global__ void __launch_bounds__(128, VIS ? 6 : MGCM_IR_SOLVE_MINB)   // 80 / 64 registers: measured best occupancy
 rt_fp64_solve(const SegTable *__restrict__ st, int col_begin, int max_nl,
               unsigned char *__restrict__ blocks, size_t stride, const double *__restrict__ ktab,
               const RtConst K, const int *__restrict__ list, const unsigned int *count,
