@@ -71,13 +71,14 @@ __global__ void rt_mixed_solve_vis(const SegTable *__restrict__ st, int col_begi
                                    const RtConst K, const int *__restrict__ list,
                                    const unsigned int *count, double *__restrict__ fl,
                                    double *__restrict__ sc);
-template <bool ONE_LEVEL>
+template <bool ONE_LEVEL, int RB>
 __global__ void rt_fp64_reduce(const SegTable *__restrict__ st, int col_begin, int col_end,
                                int max_nl, unsigned char *__restrict__ blocks, size_t stride,
                                const RtConst K, const double *__restrict__ fl_v,
                                const double *__restrict__ sc_v, const double *__restrict__ fl_i,
-                               const double *__restrict__ sc_i, uint32_t *status, int rb);
+                               const double *__restrict__ sc_i);
 size_t reduce_smem_bytes(int max_nl, int rb);
+const void *reduce_kernel(int max_nl, int rb);
 constexpr int REDUCE_WARPS = 4, REDUCE_THREADS = 32 * REDUCE_WARPS;   // rt_fp64_reduce: warp per column
 constexpr int STAGE_THREADS = 256, SCREEN_THREADS = 128;
 int reduce_rows_per_chunk(int max_nl);
@@ -555,8 +556,10 @@ int configure_kernels(int device) {
     std::lock_guard<std::mutex> lk(mu);
     if (device < 0 || device >= 256) return MGCM_RT_EINVAL;
     if (done[device]) return MGCM_RT_OK;
-    CK(cudaFuncSetAttribute(rt_fp64_reduce<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_CAP));
-    CK(cudaFuncSetAttribute(rt_fp64_reduce<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_CAP));
+    for (int nl : {32, 33})
+        for (int rb : {1, 2, 4, 8})
+            CK(cudaFuncSetAttribute(reduce_kernel(nl, rb), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)SMEM_CAP));
     CK(cudaFuncSetAttribute(rt_fp64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_CAP));
     for (int f = 0; f < 3; ++f)
         for (int q = 0; q < OC_NT; ++q)
@@ -597,8 +600,10 @@ int launch_pipeline(mgcm_rt_handle *h, Slot &sl, cudaStream_t st, int total, int
     int chunk = std::min(total, max_chunk);
     if (sl.tune.chunk > 0) chunk = std::min(chunk, sl.tune.chunk);
     const size_t n_v = (size_t)chunk * NSYS_V, n_i = (size_t)chunk * NSYS_I;
-    const size_t need = al((size_t)chunk * stride) + al(n_v * 4) + al(n_i * 4) + al(n_v * row) +
-                        al(n_i * row) + al(n_v * 32) + al(n_i * 32) + 256;
+    // flux rows and scalars in whole blocks of ROW_BLK list positions
+    const size_t r_v = row_slots(n_v), r_i = row_slots(n_i);
+    const size_t need = al((size_t)chunk * stride) + al(n_v * 4) + al(n_i * 4) + al(r_v * row) +
+                        al(r_i * row) + al(r_v * 32) + al(r_i * 32) + 256;
     (void)per_col;
     int rc = arena_ensure(h, sl.pipe, need, st);
     if (rc) return rc;
@@ -607,10 +612,10 @@ int launch_pipeline(mgcm_rt_handle *h, Slot &sl, cudaStream_t st, int total, int
     unsigned char *blocks = take((size_t)chunk * stride);
     int *list_v = reinterpret_cast<int *>(take(n_v * 4));
     int *list_i = reinterpret_cast<int *>(take(n_i * 4));
-    double *fl_v = reinterpret_cast<double *>(take(n_v * row));
-    double *fl_i = reinterpret_cast<double *>(take(n_i * row));
-    double *sc_v = reinterpret_cast<double *>(take(n_v * 32));
-    double *sc_i = reinterpret_cast<double *>(take(n_i * 32));
+    double *fl_v = reinterpret_cast<double *>(take(r_v * row));
+    double *fl_i = reinterpret_cast<double *>(take(r_i * row));
+    double *sc_v = reinterpret_cast<double *>(take(r_v * 32));
+    double *sc_i = reinterpret_cast<double *>(take(r_i * 32));
     unsigned int *counts = reinterpret_cast<unsigned int *>(take(256));
     const int rb = sl.tune.rb > 0 ? sl.tune.rb : reduce_rows_per_chunk(max_nl);
     const size_t rsm = reduce_smem_bytes(max_nl, rb);
@@ -631,8 +636,7 @@ int launch_pipeline(mgcm_rt_handle *h, Slot &sl, cudaStream_t st, int total, int
         else if (qr == 10) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&qo, rt_quad_solve<false, 10>, 128, 0);
         else if (qr == 13) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&qo, rt_quad_solve<false, 13>, 128, 0);
         sl.occ_quad = std::max(qo, 1);
-        if (max_nl <= 32) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, rt_fp64_reduce<true>, REDUCE_THREADS, rsm);
-        else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, rt_fp64_reduce<false>, REDUCE_THREADS, rsm);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, reduce_kernel(max_nl, rb), REDUCE_THREADS, rsm);
         sl.occ_screen = std::max(a, 1);
         sl.occ_solve = std::max(b, 1);
         sl.occ_reduce = std::max(c, 1);
@@ -718,12 +722,14 @@ int launch_pipeline(mgcm_rt_handle *h, Slot &sl, cudaStream_t st, int total, int
         CK(cudaEventRecord(sl.join_ev, sl.aux));
         CK(cudaStreamWaitEvent(st, sl.join_ev, 0));
         const int g3 = std::min((c1 - c0 + REDUCE_WARPS - 1) / REDUCE_WARPS, h->num_sms * sl.occ_reduce);
-        if (max_nl <= 32)
-            rt_fp64_reduce<true><<<g3, REDUCE_THREADS, rsm, st>>>(sl.d_segs, c0, c1, max_nl, blocks, stride, h->K,
-                                                                  fl_v, sc_v, fl_i, sc_i, sl.d_status, rb);
-        else
-            rt_fp64_reduce<false><<<g3, REDUCE_THREADS, rsm, st>>>(sl.d_segs, c0, c1, max_nl, blocks, stride, h->K,
-                                                                   fl_v, sc_v, fl_i, sc_i, sl.d_status, rb);
+        {
+            const SegTable *segs = sl.d_segs;
+            const RtConst &K = h->K;
+            void *args[] = {(void *)&segs, (void *)&c0, (void *)&c1, (void *)&max_nl, (void *)&blocks,
+                            (void *)&stride, (void *)&K, (void *)&fl_v, (void *)&sc_v, (void *)&fl_i,
+                            (void *)&sc_i};
+            CK(cudaLaunchKernel(reduce_kernel(max_nl, rb), dim3(g3), dim3(REDUCE_THREADS), args, rsm, st));
+        }
         nk += 5;
         CK(cudaGetLastError());
     }

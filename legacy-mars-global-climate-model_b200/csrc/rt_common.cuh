@@ -1,5 +1,6 @@
 // Device-side definitions shared by the radiation kernels.
 #pragma once
+#include <cstddef>
 #include <cstdint>
 
 namespace mgcm {
@@ -34,6 +35,20 @@ __host__ __device__ constexpr int quad_r_for(int nl) {
 }
 
 // device status bits (OR-ed into the status word)
+// Flux rows of the pipeline's solves, in blocks of 32 consecutive list
+// positions: within a block, value k (of 2 max_nl: upward then downward
+// midpoint fluxes) of the 32 systems is contiguous, so a warp of solver
+// threads stores one 256-byte segment per value, and a system's row stays
+// inside its block's 512 max_nl bytes.  Value k of position p is at
+// row_base(p, max_nl) + 32 k; scalar q (of 4) at sc_base(p) + 32 q.
+constexpr int ROW_BLK = 32;
+__host__ __device__ inline size_t row_base(size_t p, int max_nl) {
+    return (p / ROW_BLK) * (size_t)(2 * ROW_BLK * max_nl) + p % ROW_BLK;
+}
+__host__ __device__ inline size_t sc_base(size_t p) { return (p / ROW_BLK) * (size_t)(4 * ROW_BLK) + p % ROW_BLK; }
+// List positions rounded up to whole blocks (row and scalar buffer sizes).
+__host__ __device__ inline size_t row_slots(size_t n) { return (n + ROW_BLK - 1) / ROW_BLK * ROW_BLK; }
+
 constexpr uint32_t ST_PLANCK_RANGE = 1u;   // a Planck index left 1..8501 (clamped)
 constexpr uint32_t ST_NONFINITE = 2u;      // validation: NaN/Inf or p <= 0 in an input
 constexpr uint32_t ST_TEMP = 4u;           // validation: T outside [50,900)

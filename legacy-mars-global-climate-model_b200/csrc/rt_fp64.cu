@@ -202,14 +202,15 @@ rt_fp64_solve(const SegTable *__restrict__ st, int col_begin, int max_nl,
         const SegDev &sg = st->seg[si];
         const int c = g - sg.col0;
         ColSmem s = carve_smem(blocks + (size_t)(g - col_begin) * stride, max_nl, nullptr, false);
-        double *row = fl + (size_t)i * 2 * max_nl, *scr = sc + (size_t)i * 4;
+        double *row = fl + row_base(i, max_nl), *scr = sc + sc_base(i);
+        double *rdn = row + (size_t)max_nl * ROW_BLK;   // downward fluxes
         if (VIS) {
             solve_vis<2>(sg, c, sidx / D_NG + 1, sidx % D_NG + 1, sidx, s, K, ktab, w, dummy, row,
-                         row + max_nl, scr, scr + 1, scr + 2);
+                         rdn, scr, scr + ROW_BLK, scr + 2 * ROW_BLK, nullptr, ROW_BLK);
         } else {
             const int j = sidx - NSYS_V;
             solve_ir<2>(sg, c, j / D_NG + 1, j % D_NG + 1, sidx, s, K, ktab, w, dummy, row,
-                        row + max_nl, scr);
+                        rdn, scr, ROW_BLK);
         }
     }
 }
@@ -245,13 +246,15 @@ rt_quad_solve(const SegTable *__restrict__ st, int col_begin, int max_nl,
         const SegDev &sg = st->seg[find_seg(st, g)];
         const int c = g - sg.col0;
         const ColSmem s = carve_smem(blocks + (size_t)(g - col_begin) * stride, max_nl, nullptr, false);
-        double *row = fl + (size_t)ii * 2 * max_nl, *scr = sc + (size_t)ii * 4;
+        double *row = fl + row_base(ii, max_nl), *scr = sc + sc_base(ii);
+        double *rdn = row + (size_t)max_nl * ROW_BLK;   // downward fluxes
         if (VIS) {
             quad_vis<R, false>(sg, c, sidx / D_NG + 1, sidx % D_NG + 1, s, K, ktab, nullptr, live, row,
-                               row + max_nl, scr);
+                               rdn, scr, ROW_BLK);
         } else {
             const int j = sidx - NSYS_V;
-            quad_ir<R>(sg, c, j / D_NG + 1, j % D_NG + 1, s, K, ktab, live, row, row + max_nl, scr);
+            quad_ir<R>(sg, c, j / D_NG + 1, j % D_NG + 1, s, K, ktab, live, row, rdn, scr,
+                       ROW_BLK);
         }
     }
 }
@@ -268,23 +271,25 @@ template __global__ void rt_quad_solve<false, 10>(QUAD_ARGS);
 template __global__ void rt_quad_solve<false, 13>(QUAD_ARGS);
 #undef QUAD_ARGS
 
-// K3: ordered sums and heating, one warp per column.  A column's kept systems
-// sit in contiguous rows of the compact flux buffers (visible, then IR).  Lane
-// 0 streams them in chunks of `rb` rows through a ring of RED_STAGES shared
-// buffers with TMA bulk copies completed on mbarriers (next chunks in flight
-// while the current one is summed); lane j owns levels j+1, j+33, ... and sums
-// its outputs over the rows in the reference order (rows are in ascending
-// (band, Gauss) order, each scaled by the multipliers of family_multipliers).
+// K3: ordered sums and heating, one warp per column.  The solves store their
+// flux rows in blocks of 32 list positions (row_base, sc_base): value k of
+// the system at position p is fl[row_base(p) + 32 k] (k < max_nl: upward
+// midpoint flux of layer k+1; max_nl + k: downward), scalar q
+// sc[sc_base(p) + 32 q].  A column's kept systems sit in one run of
+// positions per screening group, in ascending (band, Gauss) order.  Lane j
+// owns levels j+1, j+33, ... and sums its outputs over the systems in the
+// reference order, each scaled by the multipliers of family_multipliers; the
+// loads of RB systems are issued before they are summed.
 constexpr int RED_WARPS = 4;
-constexpr int RED_STAGES = 2;
 constexpr int RED_LPL = (D_MAXNL + 1 + 31) / 32;   // levels per lane
 
-__host__ __device__ inline size_t red_warp_bytes(int max_nl, int rb) {
-    const size_t rowb = (size_t)16 * max_nl + 32;
-    size_t b = (size_t)RED_STAGES * rb * rowb;        // ring
-    b += (size_t)3 * NSYS * 8;                        // multipliers
+// Shared memory of one warp: the multipliers of both families, FMNET per
+// level of both families, the top-of-atmosphere values, and one family's
+// kept list positions in order.
+__host__ __device__ inline size_t red_warp_bytes() {
+    size_t b = (size_t)3 * NSYS * 8;                  // multipliers
     b += (size_t)2 * (D_MAXNL + 2) * 8 + 4 * 8;       // FMNET per level, top values
-    b += (size_t)RED_STAGES * 8;                      // mbarriers
+    b += (size_t)NSYS * 4;                            // list positions
     return (b + 127) / 128 * 128;
 }
 
@@ -344,27 +349,20 @@ __device__ inline void warp_multipliers(const unsigned char *skip, bool day, con
     p3[pos] = 1.0;
 }
 
-template <bool ONE_LEVEL>   // max NL <= 32: one level per lane
+template <bool ONE_LEVEL, int RB>   // ONE_LEVEL: max NL <= 32, one level per lane
 __global__ void __launch_bounds__(32 * RED_WARPS)
 rt_fp64_reduce(const SegTable *__restrict__ st, int col_begin, int col_end, int max_nl,
                unsigned char *__restrict__ blocks, size_t stride, const RtConst K,
                const double *__restrict__ fl_v, const double *__restrict__ sc_v,
-               const double *__restrict__ fl_i, const double *__restrict__ sc_i,
-               uint32_t *status, int rb) {
+               const double *__restrict__ fl_i, const double *__restrict__ sc_i) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
+    constexpr int LPL = ONE_LEVEL ? 1 : RED_LPL;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const size_t row = (size_t)2 * max_nl;   // doubles per compact row
-    const uint32_t rowb = (uint32_t)(row * 8), chunkb = (uint32_t)rb * (rowb + 32);
-    unsigned char *ws = smem_raw + (size_t)wid * red_warp_bytes(max_nl, rb);
-    unsigned char *ring = ws;
-    double *m1 = reinterpret_cast<double *>(ws + (size_t)RED_STAGES * chunkb);
+    unsigned char *ws = smem_raw + (size_t)wid * red_warp_bytes();
+    double *m1 = reinterpret_cast<double *>(ws);
     double *m2 = m1 + NSYS, *m3 = m2 + NSYS;
     double *fmv = m3 + NSYS, *fmi = fmv + (D_MAXNL + 2), *misc = fmi + (D_MAXNL + 2);
-    uint64_t *bar = reinterpret_cast<uint64_t *>(misc + 4);
-    if (lane == 0)
-        for (int k = 0; k < RED_STAGES; ++k) mbar_init(&bar[k], 1);
-    __syncwarp();
-    unsigned int gf = 0, gc = 0;   // chunks issued / consumed by this warp
+    int *rpos = reinterpret_cast<int *>(misc + 4);
 
     for (int g = col_begin + blockIdx.x * RED_WARPS + wid; g < col_end; g += gridDim.x * RED_WARPS) {
         const int si = find_seg(st, g);
@@ -373,82 +371,92 @@ rt_fp64_reduce(const SegTable *__restrict__ st, int col_begin, int col_end, int 
         const int NL = sg.L + 1;
         const ColSmem s = carve_smem(blocks + (size_t)(g - col_begin) * stride, max_nl, nullptr, false);
         const bool day = sg.acosz[c] >= R4(1.0e-5);
-        // kept rows per screening group (visible groups empty at night)
-        int gbase[SCREEN_GROUPS], gcnt[SCREEN_GROUPS], nch = 0;
-#pragma unroll
-        for (int w = 0; w < SCREEN_GROUPS; ++w) {
-            gbase[w] = s.meta[2 * w];
-            gcnt[w] = (w < SCREEN_GROUPS_V && !day) ? 0 : s.meta[2 * w + 1];
-            nch += (gcnt[w] + rb - 1) / rb;
-        }
-        // chunk j -> family, first list position, family row index, rows
-        auto chunk = [&](int j, bool &vis, int &b0, int &fr, int &cnt) {
-            int off = 0;
-#pragma unroll
-            for (int w = 0; w < SCREEN_GROUPS; ++w) {
-                if (w == SCREEN_GROUPS_V) off = 0;
-                const int nc = (gcnt[w] + rb - 1) / rb;
-                if (j >= 0 && j < nc) {
-                    vis = w < SCREEN_GROUPS_V;
-                    b0 = gbase[w] + j * rb;
-                    fr = off + j * rb;
-                    cnt = min(rb, gcnt[w] - j * rb);
-                }
-                j -= nc;
-                off += gcnt[w];
-            }
-        };
-        auto issue = [&](int j) {
-            if (lane == 0) {
-                bool vis = true;
-                int b0 = 0, fr = 0, cnt = 0;
-                chunk(j, vis, b0, fr, cnt);
-                unsigned char *dst = ring + (size_t)(gf % RED_STAGES) * chunkb;
-                fence_proxy_async_smem();
-                mbar_arrive_expect_tx(&bar[gf % RED_STAGES], (uint32_t)cnt * (rowb + 32));
-                bulk_g2s(dst, (vis ? fl_v : fl_i) + (size_t)b0 * row, (uint32_t)cnt * rowb,
-                         &bar[gf % RED_STAGES]);
-                bulk_g2s(dst + (size_t)rb * rowb, (vis ? sc_v : sc_i) + (size_t)b0 * 4,
-                         (uint32_t)cnt * 32, &bar[gf % RED_STAGES]);
-            }
-            ++gf;
-        };
-        int next = 0;
-        while (next < nch && gf - gc < RED_STAGES) issue(next++);
         warp_multipliers(s.skip, day, K, m1, m2, m3);
-        __syncwarp();
-
-        double acc[3][RED_LPL], top = 0.0, dif = 0.0;
-        auto clear = [&]() {
-#pragma unroll
-            for (int q = 0; q < 3; ++q)
-#pragma unroll
-                for (int r = 0; r < RED_LPL; ++r) acc[q][r] = 0.0;
-            top = 0.0;
-            dif = 0.0;
-        };
-        // family outputs, FMNET kept for the heating
-        auto flush = [&](bool vis) {
-#pragma unroll
-            for (int r = 0; r < RED_LPL; ++r) {
+        for (int fam = 0; fam < 2; ++fam) {
+            const bool vis = fam == 0;
+            // list positions of the family's kept systems (none at night for
+            // the visible family: its outputs are zeros)
+            int nrow = 0;
+            if (!vis || day) {
+                const int w0 = vis ? 0 : SCREEN_GROUPS_V, w1 = vis ? SCREEN_GROUPS_V : SCREEN_GROUPS;
+                for (int gw = w0; gw < w1; ++gw) {
+                    const int gb = s.meta[2 * gw], gn = s.meta[2 * gw + 1];
+                    for (int q = lane; q < gn; q += 32) rpos[nrow + q] = gb + q;
+                    nrow += gn;
+                }
+            }
+            __syncwarp();
+            const double *fl = vis ? fl_v : fl_i, *sc = vis ? sc_v : sc_i;
+            const double *f1 = vis ? m1 : m1 + NSYS_V, *f2 = vis ? m2 : m2 + NSYS_V, *f3 = vis ? m3 : m3 + NSYS_V;
+            double top = 0.0, dif = 0.0;
+#pragma unroll 1
+            for (int r = 0; r < LPL; ++r) {
+                if (32 * r >= NL) break;
                 const int l = lane + 1 + 32 * r;
-                if (l > NL) break;
-                const size_t o = (size_t)c * NL + l - 1;
-                if (vis) {
-                    sg.fmnetv[o] = acc[0][r];
-                    sg.fluxupv[o] = acc[1][r];
-                    sg.fluxdnv[o] = acc[2][r];
-                    fmv[l] = acc[0][r];
-                    if (l == NL) {
-                        sg.dnvflux[c] = acc[2][r];
-                        sg.fluxsurf[c] = (1.0 - sg.als[c]) * acc[2][r];
+                const bool lv = l <= NL;
+                const size_t ou = (size_t)(lv ? l - 1 : 0) * ROW_BLK, od = ou + (size_t)max_nl * ROW_BLK;
+                double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+                for (int f0 = 0; f0 < nrow; f0 += RB) {
+                    double up[RB], dn[RB], t0[RB], t1[RB];
+#pragma unroll
+                    for (int q = 0; q < RB; ++q) {
+                        up[q] = dn[q] = t0[q] = t1[q] = 0.0;
+                        if (f0 + q < nrow) {
+                            const int p = rpos[f0 + q];
+                            const double *pr = fl + row_base(p, max_nl);
+                            if (lv) {
+                                up[q] = __ldg(pr + ou);
+                                dn[q] = __ldg(pr + od);
+                            }
+                            if (r == 0) {
+                                const double *ps = sc + sc_base(p);
+                                t0[q] = vis ? __ldg(ps) - __ldg(ps + ROW_BLK) : __ldg(ps);
+                                if (vis) t1[q] = __ldg(ps + 2 * ROW_BLK);
+                            }
+                        }
                     }
-                } else {
-                    sg.fmneti[o] = acc[0][r];
-                    sg.fluxupi[o] = acc[1][r];
-                    sg.fluxdni[o] = acc[2][r];
-                    fmi[l] = acc[0][r];
-                    if (l == NL) sg.dnirflux[c] = acc[2][r];
+#pragma unroll
+                    for (int q = 0; q < RB; ++q) {
+                        if (f0 + q < nrow) {
+                            const double a = f1[f0 + q], b = f2[f0 + q], e = f3[f0 + q];
+                            // ((v*a)*b)*e in the reference order; a factor that is
+                            // exactly 1.0 leaves the product unchanged and is
+                            // skipped (warp-uniform)
+                            const bool b1 = b == 1.0, e1 = e == 1.0;
+                            auto wt = [&](double v) {
+                                double x = v * a;
+                                if (!b1) x = x * b;
+                                if (!e1) x = x * e;
+                                return x;
+                            };
+                            a0 = a0 + wt(up[q] - dn[q]);
+                            a1 = a1 + wt(up[q]);
+                            a2 = a2 + wt(dn[q]);
+                            if (r == 0) {
+                                top = top + wt(t0[q]);
+                                if (vis) dif = dif + wt(t1[q]);
+                            }
+                        }
+                    }
+                }
+                if (lv) {
+                    const size_t o = (size_t)c * NL + l - 1;
+                    if (vis) {
+                        sg.fmnetv[o] = a0;
+                        sg.fluxupv[o] = a1;
+                        sg.fluxdnv[o] = a2;
+                        fmv[l] = a0;
+                        if (l == NL) {
+                            sg.dnvflux[c] = a2;
+                            sg.fluxsurf[c] = (1.0 - sg.als[c]) * a2;
+                        }
+                    } else {
+                        sg.fmneti[o] = a0;
+                        sg.fluxupi[o] = a1;
+                        sg.fluxdni[o] = a2;
+                        fmi[l] = a0;
+                        if (l == NL) sg.dnirflux[c] = a2;
+                    }
                 }
             }
             if (lane == 0) {
@@ -462,75 +470,8 @@ rt_fp64_reduce(const SegTable *__restrict__ st, int col_begin, int col_end, int 
                     misc[1] = top;
                 }
             }
-        };
-        clear();
-        bool cur_vis = true;
-        for (int j = 0; j < nch; ++j) {
-            bool vis = true;
-            int b0 = 0, r0 = 0, cnt = 0;
-            chunk(j, vis, b0, r0, cnt);
-            if (vis != cur_vis) {   // visible rows done
-                flush(true);
-                clear();
-                cur_vis = false;
-            }
-            const unsigned int stg = gc % RED_STAGES;
-            if (!mbar_wait(&bar[stg], (gc / RED_STAGES) & 1u, status)) {
-                for (++gc; gc < gf; ++gc) mbar_wait(&bar[gc % RED_STAGES], (gc / RED_STAGES) & 1u, status);
-                return;   // copies drained; status holds the error
-            }
-            const double *buf = reinterpret_cast<const double *>(ring + (size_t)stg * chunkb);
-            const double *scb = reinterpret_cast<const double *>(ring + (size_t)stg * chunkb + (size_t)rb * rowb);
-            const double *f1 = (vis ? m1 : m1 + NSYS_V) + r0, *f2 = (vis ? m2 : m2 + NSYS_V) + r0,
-                         *f3 = (vis ? m3 : m3 + NSYS_V) + r0;
-            for (int k = 0; k < cnt; ++k) {
-                const double a = f1[k], b = f2[k], e = f3[k];
-                // ((v*a)*b)*e in the reference order; a factor that is exactly
-                // 1.0 leaves the product unchanged and is skipped (warp-uniform)
-                const bool b1 = b == 1.0, e1 = e == 1.0;
-                auto wt = [&](double v) {
-                    double x = v * a;
-                    if (!b1) x = x * b;
-                    if (!e1) x = x * e;
-                    return x;
-                };
-                const double *pr = buf + (size_t)k * row;
-                if (ONE_LEVEL) {
-                    if (lane < NL) {
-                        const double up = pr[lane], dn = pr[max_nl + lane];
-                        acc[0][0] = acc[0][0] + wt(up - dn);
-                        acc[1][0] = acc[1][0] + wt(up);
-                        acc[2][0] = acc[2][0] + wt(dn);
-                    }
-                } else {
-#pragma unroll
-                    for (int r = 0; r < RED_LPL; ++r) {
-                        const int l = lane + 1 + 32 * r;
-                        if (l > NL) break;
-                        const double up = pr[l - 1], dn = pr[max_nl + l - 1];
-                        acc[0][r] = acc[0][r] + wt(up - dn);
-                        acc[1][r] = acc[1][r] + wt(up);
-                        acc[2][r] = acc[2][r] + wt(dn);
-                    }
-                }
-                const double *sk = scb + (size_t)k * 4;
-                if (vis) {
-                    top = top + wt(sk[0] - sk[1]);
-                    dif = dif + wt(sk[2]);
-                } else {
-                    top = top + wt(sk[0]);
-                }
-            }
-            ++gc;
-            __syncwarp();
-            if (next < nch) issue(next++);
+            __syncwarp();   // rpos is rewritten by the next family
         }
-        if (cur_vis) {   // no IR chunk followed: visible outputs (zeros at night)
-            flush(true);
-            clear();
-        }
-        flush(false);
-        __syncwarp();
         // divergences and heating rates (code/comp3.f:677-681,735-738,765-771)
         const double *plev = sg.plev + (size_t)c * (2 * sg.L + 3);
         const int LEV = 2 * sg.L + 3;
@@ -548,23 +489,43 @@ rt_fp64_reduce(const SegTable *__restrict__ st, int col_begin, int col_end, int 
             sg.irtotal[o] = irt;
             sg.qrad[o] = (sunlte + irt) / (735.94 * ym * om);
         }
-        __syncwarp();
+        __syncwarp();   // fmv, fmi, misc and the multipliers are rewritten by the next column
     }
 }
 
 #define REDUCE_ARGS                                                                                    \
     const SegTable *__restrict__, int, int, int, unsigned char *__restrict__, size_t, const RtConst,  \
         const double *__restrict__, const double *__restrict__, const double *__restrict__,          \
-        const double *__restrict__, uint32_t *, int
-template __global__ void rt_fp64_reduce<true>(REDUCE_ARGS);
-template __global__ void rt_fp64_reduce<false>(REDUCE_ARGS);
+        const double *__restrict__
+#define REDUCE_INST(RB)                                              \
+    template __global__ void rt_fp64_reduce<true, RB>(REDUCE_ARGS);  \
+    template __global__ void rt_fp64_reduce<false, RB>(REDUCE_ARGS);
+REDUCE_INST(1)
+REDUCE_INST(2)
+REDUCE_INST(4)
+REDUCE_INST(8)
+#undef REDUCE_INST
 #undef REDUCE_ARGS
 
-// Shared memory of rt_fp64_reduce with `rb` rows per chunk.
-size_t reduce_smem_bytes(int max_nl, int rb) { return (size_t)RED_WARPS * red_warp_bytes(max_nl, rb); }
+// Shared memory of rt_fp64_reduce (the same for every batch size).
+size_t reduce_smem_bytes(int max_nl, int rb) {
+    (void)max_nl;
+    (void)rb;
+    return (size_t)RED_WARPS * red_warp_bytes();
+}
+// Systems whose loads the reduce issues before it sums them, by default.
 int reduce_rows_per_chunk(int max_nl) {
-    const int rowb = 16 * max_nl + 32;
-    return std::max(1, std::min(8, 2048 / rowb));
+    (void)max_nl;
+    return 4;
+}
+// The reduce kernel of a launch: one level per lane up to NL = 32, and RB
+// in {1, 2, 4, 8} (other values round down).
+const void *reduce_kernel(int max_nl, int rb) {
+    const bool one = max_nl <= 32;
+    if (rb >= 8) return one ? (const void *)rt_fp64_reduce<true, 8> : (const void *)rt_fp64_reduce<false, 8>;
+    if (rb >= 4) return one ? (const void *)rt_fp64_reduce<true, 4> : (const void *)rt_fp64_reduce<false, 4>;
+    if (rb >= 2) return one ? (const void *)rt_fp64_reduce<true, 2> : (const void *)rt_fp64_reduce<false, 2>;
+    return one ? (const void *)rt_fp64_reduce<true, 1> : (const void *)rt_fp64_reduce<false, 1>;
 }
 
 // Partial radiation: DIRECTSOL from DETAU (code/dsolflux.f:28-45) and

@@ -169,12 +169,14 @@ __device__ __forceinline__ float taugas_f(const ColSmem &s, int k, const float *
 // MODE 0: whole system (fused kernel); 1: screen only (optics, TLIMIT
 // decision, DETAU and CUMTAUV); 2: solve a system the screen kept.
 // F32: opacities from the FP32 table of Cmk*k (mixed precision); everything
-// after the per-level optical depth stays FP64.
+// after the per-level optical depth stays FP64.  The midpoint fluxes of layer
+// n go to fmp[(n-1) rs] and fmm[(n-1) rs].
 template <int MODE, bool F32 = false>
 __device__ void solve_vis(const SegDev &sg, int c, int nw, int ng, int sidx, ColSmem &s,
                           const RtConst &K, const double *__restrict__ kv, SysLocal &w,
                           unsigned int &nsolved, double *fmp, double *fmm, double *sc0,
-                          double *sc1, double *sc2, const float *__restrict__ kvf = nullptr) {
+                          double *sc1, double *sc2, const float *__restrict__ kvf = nullptr,
+                          size_t rs = 1) {
     const int L = sg.L, NL = L + 1;
     const double fz0 = K.fzerov[nw - 1];
     const bool band_skip = ng < D_NG && fz0 >= R4(0.99);
@@ -346,9 +348,9 @@ __device__ void solve_vis(const SegDev &sg, int c, int nw, int ng, int sidx, Col
             const double em = 1.0 / ep;
             const double et = mgcm_rt_exp(-dmin(a4n / u0, MAXEXP));
             const double cpmid = ap * et, cmmid = am * et;
-            fmp[n - 1] = xk1 * ep + gama * xk2 * em + cpmid;
+            fmp[(size_t)(n - 1) * rs] = xk1 * ep + gama * xk2 * em + cpmid;
             double m = xk1 * ep * gama + xk2 * em + cmmid;
-            fmm[n - 1] = m + u0 * f0pi * et;
+            fmm[(size_t)(n - 1) * rs] = m + u0 * f0pi * et;
         } else {
             const double tb = w.a3[NL + 1];
             const double ep = mgcm_rt_exp(dmin(TAUMAX, lam * (tb - a3n)));
@@ -356,10 +358,10 @@ __device__ void solve_vis(const SegDev &sg, int c, int nw, int ng, int sidx, Col
             const double taumid = dmin(tb, TAUMAX);
             const double et = mgcm_rt_exp(-dmin(taumid / u0, MAXEXP));
             const double cpmid = ap * et, cmmid = am * et;
-            fmp[n - 1] = xk1 * ep + gama * xk2 * em + cpmid;
+            fmp[(size_t)(n - 1) * rs] = xk1 * ep + gama * xk2 * em + cpmid;
             const double m = xk1 * ep * gama + xk2 * em + cmmid;
             *sc2 = m;
-            fmm[n - 1] = m + u0 * f0pi * et;
+            fmm[(size_t)(n - 1) * rs] = m + u0 * f0pi * et;
         }
     }
 }
@@ -370,10 +372,11 @@ __device__ void solve_vis(const SegDev &sg, int c, int nw, int ng, int sidx, Col
 #endif
 constexpr int IR_SCREEN_UNROLL = MGCM_IR_SCREEN_UNROLL;
 
+// The midpoint fluxes of layer n go to fmp[(n-1) rs] and fmm[(n-1) rs].
 template <int MODE>
 __device__ void solve_ir(const SegDev &sg, int c, int nw, int ng, int sidx, ColSmem &s,
                          const RtConst &K, const double *__restrict__ ki, SysLocal &w,
-                         unsigned int &nsolved, double *fmp, double *fmm, double *sc0) {
+                         unsigned int &nsolved, double *fmp, double *fmm, double *sc0, size_t rs = 1) {
     const int L = sg.L, NL = L + 1, LEV = 2 * L + 3;
     const double fz0 = K.fzeroi[nw - 1];
     if (ng < D_NG && fz0 >= R4(0.99)) {
@@ -537,8 +540,8 @@ __device__ void solve_ir(const SegDev &sg, int c, int nw, int ng, int sidx, ColS
         const double cmmid = b0 + b1 * dtk - b1 * term;
         const double p = xk1 * ep + gama * xk2 * em + cpmid;
         const double m = xk1 * ep * gama + xk2 * em + cmmid;
-        fmp[n - 1] = p * PI_D;
-        fmm[n - 1] = m * PI_D;
+        fmp[(size_t)(n - 1) * rs] = p * PI_D;
+        fmm[(size_t)(n - 1) * rs] = m * PI_D;
         if (n == 1) {
             const double ep1 = 1.0, em1 = 1.0;
             const double cpm = b0 + b1 * term, cmm = b0 - b1 * term;

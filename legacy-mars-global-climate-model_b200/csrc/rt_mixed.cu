@@ -35,9 +35,11 @@ rt_mixed_solve_vis(const SegTable *__restrict__ st, int col_begin, int max_nl,
         const SegDev &sg = st->seg[find_seg(st, g)];
         const int c = g - sg.col0;
         ColSmem s = carve_smem(blocks + (size_t)(g - col_begin) * stride, max_nl, nullptr, false);
-        double *row = fl + (size_t)i * 2 * max_nl, *scr = sc + (size_t)i * 4;
+        double *row = fl + row_base(i, max_nl), *scr = sc + sc_base(i);
+        double *rdn = row + (size_t)max_nl * ROW_BLK;   // downward fluxes
         fp64::solve_vis<2, true>(sg, c, sidx / D_NG + 1, sidx % D_NG + 1, sidx, s, K, ktab, w,
-                                 dummy, row, row + max_nl, scr, scr + 1, scr + 2, ktabf);
+                                 dummy, row, rdn, scr, scr + ROW_BLK, scr + 2 * ROW_BLK, ktabf,
+                                 ROW_BLK);
     }
 }
 
@@ -61,9 +63,10 @@ rt_quad_mixed_vis(const SegTable *__restrict__ st, int col_begin, int max_nl,
         const SegDev &sg = st->seg[find_seg(st, g)];
         const int c = g - sg.col0;
         const ColSmem s = carve_smem(blocks + (size_t)(g - col_begin) * stride, max_nl, nullptr, false);
-        double *row = fl + (size_t)ii * 2 * max_nl, *scr = sc + (size_t)ii * 4;
+        double *row = fl + row_base(ii, max_nl), *scr = sc + sc_base(ii);
+        double *rdn = row + (size_t)max_nl * ROW_BLK;   // downward fluxes
         fp64::quad_vis<R, true>(sg, c, sidx / D_NG + 1, sidx % D_NG + 1, s, K, ktab, ktabf, live, row,
-                                row + max_nl, scr);
+                                rdn, scr, ROW_BLK);
     }
 }
 

@@ -23,13 +23,16 @@ rt_solve_oc(const SegTable *__restrict__ st, int col_begin, int max_nl, unsigned
         const SegDev &sg = st->seg[find_seg(st, g)];
         const int c = g - sg.col0;
         const ColSmem s = carve_smem(blocks + (size_t)(g - col_begin) * stride, max_nl, nullptr, false);
-        double *row = fl + (size_t)i * 2 * max_nl, *scr = sc + (size_t)i * 4;
+        double *row = fl + row_base(i, max_nl), *scr = sc + sc_base(i);
+        double *rdn = row + (size_t)max_nl * ROW_BLK;   // downward fluxes
         if (VIS) {
             onchip::solve_vis_oc<onchip::SmemSlots<T>, F32>(sg, c, sidx / D_NG + 1, sidx % D_NG + 1, s, K, ktab,
-                                                            ktabf, ss, row, row + max_nl, scr, scr + 1, scr + 2);
+                                                            ktabf, ss, row, rdn, scr, scr + ROW_BLK,
+                                                            scr + 2 * ROW_BLK, ROW_BLK);
         } else {
             const int j = sidx - NSYS_V;
-            onchip::solve_ir_oc(sg, c, j / D_NG + 1, j % D_NG + 1, s, ktab, ss, row, row + max_nl, scr);
+            onchip::solve_ir_oc(sg, c, j / D_NG + 1, j % D_NG + 1, s, ktab, ss, row, rdn, scr,
+                                ROW_BLK);
         }
     }
 }
@@ -67,14 +70,16 @@ rt_solve_tm(const SegTable *__restrict__ st, int col_begin, int max_nl, unsigned
         const SegDev &sg = st->seg[find_seg(st, g)];
         const int c = g - sg.col0;
         const ColSmem s = carve_smem(blocks + (size_t)(g - col_begin) * stride, max_nl, nullptr, false);
-        double *row = fl + (size_t)i * 2 * max_nl, *scr = sc + (size_t)i * 4;
+        double *row = fl + row_base(i, max_nl), *scr = sc + sc_base(i);
+        double *rdn = row + (size_t)max_nl * ROW_BLK;   // downward fluxes
         if (VIS) {
             onchip::solve_vis_oc<onchip::HybridSlots<T>, F32>(sg, c, sidx / D_NG + 1, sidx % D_NG + 1, s, K,
-                                                              ktab, ktabf, ss, row, row + max_nl, scr, scr + 1,
-                                                              scr + 2);
+                                                              ktab, ktabf, ss, row, rdn, scr,
+                                                              scr + ROW_BLK, scr + 2 * ROW_BLK, ROW_BLK);
         } else {
             const int j = sidx - NSYS_V;
-            onchip::solve_ir_oc(sg, c, j / D_NG + 1, j % D_NG + 1, s, ktab, ss, row, row + max_nl, scr);
+            onchip::solve_ir_oc(sg, c, j / D_NG + 1, j % D_NG + 1, s, ktab, ss, row, rdn, scr,
+                                ROW_BLK);
         }
     }
     tmem_fence_before_sync();

@@ -66,7 +66,7 @@ struct HybridSlots {
 // ---------------------------------------------------------------- infrared
 template <class S>
 __device__ void solve_ir_oc(const SegDev &sg, int c, int nw, int ng, const ColSmem &s, const double *__restrict__ ki,
-                            const S &st, double *fmp, double *fmm, double *sc0) {
+                            const S &st, double *fmp, double *fmm, double *sc0, size_t rs) {
     const int L = sg.L, NL = L + 1, LEV = 2 * L + 3;
     const int oW = 0, oDT = NL, oTK = 2 * NL, oAS = 3 * NL, oDS = 5 * NL;   // AS(r) at oAS + r-1
     const double *tb = ki + (size_t)(nw - 1) * D_NT * D_NP * D_NH * D_NGK + (ng - 1);
@@ -193,8 +193,8 @@ __device__ void solve_ir_oc(const SegDev &sg, int c, int nw, int ng, const ColSm
         const double cmmid = b0 + b1 * dtk - b1 * term;
         const double p = xk1 * ep + gama * xk2 * em + cpmid;
         const double m = xk1 * ep * gama + xk2 * em + cmmid;
-        fmp[n - 1] = p * PI_D;
-        fmm[n - 1] = m * PI_D;
+        fmp[(size_t)(n - 1) * rs] = p * PI_D;
+        fmm[(size_t)(n - 1) * rs] = m * PI_D;
         if (n == 1) {
             const double ep1 = 1.0, em1 = 1.0;
             const double cpm = b0 + b1 * term, cmm = b0 - b1 * term;
@@ -210,7 +210,7 @@ __device__ void solve_ir_oc(const SegDev &sg, int c, int nw, int ng, const ColSm
 template <class S, bool F32>
 __device__ void solve_vis_oc(const SegDev &sg, int c, int nw, int ng, const ColSmem &s, const RtConst &K,
                              const double *__restrict__ kv, const float *__restrict__ kvf, const S &st,
-                             double *fmp, double *fmm, double *sc0, double *sc1, double *sc2) {
+                             double *fmp, double *fmm, double *sc0, double *sc1, double *sc2, size_t rs) {
     const int L = sg.L, NL = L + 1;
     const int oW = 0, oDL = NL, oTAU = 2 * NL, oTCM = 3 * NL + 1, oAS = 4 * NL + 1, oDS = 6 * NL + 1;
     const double *tb = kv + (size_t)(nw - 1) * D_NT * D_NP * D_NH * D_NGK + (ng - 1);
@@ -371,19 +371,19 @@ __device__ void solve_vis_oc(const SegDev &sg, int c, int nw, int ng, const ColS
             const double em = 1.0 / ep;
             const double et = mgcm_rt_exp(-dmin(a4n / u0, MAXEXP));
             const double cpmid = ap * et, cmmid = am * et;
-            fmp[n - 1] = xk1 * ep + gama * xk2 * em + cpmid;
+            fmp[(size_t)(n - 1) * rs] = xk1 * ep + gama * xk2 * em + cpmid;
             double m = xk1 * ep * gama + xk2 * em + cmmid;
-            fmm[n - 1] = m + u0 * f0pi * et;
+            fmm[(size_t)(n - 1) * rs] = m + u0 * f0pi * et;
         } else {
             const double ep = mgcm_rt_exp(dmin(TAUMAX, lam * (tbot - a3n)));
             const double em = 1.0 / ep;
             const double taumid = dmin(tbot, TAUMAX);
             const double et = mgcm_rt_exp(-dmin(taumid / u0, MAXEXP));
             const double cpmid = ap * et, cmmid = am * et;
-            fmp[n - 1] = xk1 * ep + gama * xk2 * em + cpmid;
+            fmp[(size_t)(n - 1) * rs] = xk1 * ep + gama * xk2 * em + cpmid;
             const double m = xk1 * ep * gama + xk2 * em + cmmid;
             *sc2 = m;
-            fmm[n - 1] = m + u0 * f0pi * et;
+            fmm[(size_t)(n - 1) * rs] = m + u0 * f0pi * et;
         }
     }
 }

@@ -32,7 +32,7 @@ template <int R, bool F32>
 __device__ __forceinline__ void quad_vis(const SegDev &sg, int c, int nw, int ng, const ColSmem &s,
                                          const RtConst &K, const double *__restrict__ kv,
                                          const float *__restrict__ kvf, bool live, double *fmp,
-                                         double *fmm, double *scr) {
+                                         double *fmm, double *scr, size_t rs = 1) {
     const int q = threadIdx.x & 3;
     const int L = sg.L, NL = L + 1;
     const int Rr = (NL + 3) / 4;
@@ -237,15 +237,15 @@ __device__ __forceinline__ void quad_vis(const SegDev &sg, int c, int nw, int ng
                     double fdn = xk1 * e1 * gama + xk2 * e2 + am[j];
                     fdn = fdn + u0 * f0pi * mgcm_rt_exp(-dmin(0.0 / u0, MAXEXP));
                     scr[0] = fup;
-                    scr[1] = fdn;
+                    scr[rs] = fdn;
                 }
                 const double cpmid = ap[j] * ett[j], cmmid = am[j] * ett[j];
                 const double p = xk1 * ep[j] + gama * xk2 * em[j] + cpmid;
                 const double m = xk1 * ep[j] * gama + xk2 * em[j] + cmmid;
                 if (live) {
-                    fmp[l - 1] = p;
-                    fmm[l - 1] = m + u0 * f0pi * ett[j];
-                    if (l == NL) scr[2] = m;
+                    fmp[(size_t)(l - 1) * rs] = p;
+                    fmm[(size_t)(l - 1) * rs] = m + u0 * f0pi * ett[j];
+                    if (l == NL) scr[2 * rs] = m;
                 }
                 if (l < NL) xa = dsh[j] - ash[j] * xb;
             }
@@ -258,7 +258,7 @@ __device__ __forceinline__ void quad_vis(const SegDev &sg, int c, int nw, int ng
 template <int R>
 __device__ __forceinline__ void quad_ir(const SegDev &sg, int c, int nw, int ng, const ColSmem &s,
                                         const RtConst &K, const double *__restrict__ ki, bool live,
-                                        double *fmp, double *fmm, double *scr) {
+                                        double *fmp, double *fmm, double *scr, size_t rs = 1) {
     const int q = threadIdx.x & 3;
     const int L = sg.L, NL = L + 1, LEV = 2 * L + 3;
     const int Rr = (NL + 3) / 4;
@@ -434,8 +434,8 @@ __device__ __forceinline__ void quad_ir(const SegDev &sg, int c, int nw, int ng,
                 const double p = xk1 * ep[j] + gama * xk2 * em[j] + lam[j];
                 const double m = xk1 * ep[j] * gama + xk2 * em[j] + a4[j];
                 if (live) {
-                    fmp[l - 1] = p * PI_D;
-                    fmm[l - 1] = m * PI_D;
+                    fmp[(size_t)(l - 1) * rs] = p * PI_D;
+                    fmm[(size_t)(l - 1) * rs] = m * PI_D;
                     if (l == 1) {
                         const double b0 = s.b0_i[l * D_NI + nw - 1], b1 = b1v[j];
                         const double e1 = 1.0, e2 = 1.0;
