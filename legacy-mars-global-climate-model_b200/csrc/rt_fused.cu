@@ -54,16 +54,16 @@ __host__ __device__ inline size_t fused_smem_bytes(int warps, int tc) {
 }
 
 // Global scratch of one buffer: TC column blocks and the flux rows of every
-// system a tile can keep; a CTA holds two.
+// system a tile can keep (whole blocks of ROW_BLK rows); a CTA holds two.
 __host__ __device__ inline size_t fused_buf_bytes(int tc, int max_nl, size_t stride) {
     const size_t row = (size_t)2 * max_nl * 8;
-    return ((size_t)tc * stride + (size_t)tc * NSYS * (row + 32) + 255) / 256 * 256;
+    return ((size_t)tc * stride + row_slots((size_t)tc * NSYS) * (row + 32) + 255) / 256 * 256;
 }
 
 // One tile in one buffer.
 struct FzBuf {
     unsigned char *blocks;   // TC column blocks
-    double *fl, *sc;         // flux rows [TC * NSYS][2 max_nl], scalars [TC * NSYS][4]
+    double *fl, *sc;         // flux rows and scalars of the solve order (row_base, sc_base)
     int *list;               // kept systems: visible from 0 up, IR from TC*NSYS-1 down
     int g0, ng;              // first global column, columns (0: no tile)
 };
@@ -123,13 +123,13 @@ __device__ __forceinline__ void fz_screen_item(const SegTable *__restrict__ st, 
 }
 
 // Solve kept system i of a tile (visible entries [0, nv), IR after), one
-// thread; rows: visible at list position, IR at TC * NSYS_V + position.
+// thread; its flux row is row i, so the 32 threads of a warp, which take 32
+// consecutive systems, store one 256-byte segment per value.
 template <bool F32, int TC>
 __device__ __forceinline__ void fz_solve_one(const SegTable *__restrict__ st, const RtConst &K,
                                              const double *__restrict__ kv, const double *__restrict__ ki,
                                              const float *__restrict__ kvf, const FzBuf &b, int i, int nv,
                                              int max_nl, size_t stride, SysLocal &w) {
-    const size_t row = (size_t)2 * max_nl;
     const bool vis = i < nv;
     const int li = vis ? i : i - nv;
     const int e = b.list[vis ? li : TC * NSYS - 1 - li];
@@ -137,15 +137,15 @@ __device__ __forceinline__ void fz_solve_one(const SegTable *__restrict__ st, co
     const SegDev &sg = st->seg[find_seg(st, g)];
     const int c = g - sg.col0;
     ColSmem s = carve_smem(b.blocks + (size_t)j * stride, max_nl, nullptr, false);
-    const size_t r = vis ? (size_t)li : (size_t)TC * NSYS_V + li;
-    double *fr = b.fl + r * row, *scr = b.sc + r * 4;
+    double *fr = b.fl + row_base(i, max_nl), *scr = b.sc + sc_base(i);
+    double *fdn = fr + (size_t)max_nl * ROW_BLK;
     unsigned int dummy = 0;
     if (vis) {
-        solve_vis<2, F32>(sg, c, sidx / D_NG + 1, sidx % D_NG + 1, sidx, s, K, kv, w, dummy, fr, fr + max_nl, scr,
-                          scr + 1, scr + 2, kvf);
+        solve_vis<2, F32>(sg, c, sidx / D_NG + 1, sidx % D_NG + 1, sidx, s, K, kv, w, dummy, fr, fdn, scr,
+                          scr + ROW_BLK, scr + 2 * ROW_BLK, kvf, ROW_BLK);
     } else {
         const int jj = sidx - NSYS_V;
-        solve_ir<2>(sg, c, jj / D_NG + 1, jj % D_NG + 1, sidx, s, K, ki, w, dummy, fr, fr + max_nl, scr);
+        solve_ir<2>(sg, c, jj / D_NG + 1, jj % D_NG + 1, sidx, s, K, ki, w, dummy, fr, fdn, scr, ROW_BLK);
     }
 }
 
@@ -161,8 +161,7 @@ __device__ __forceinline__ void fz_solve_one(const SegTable *__restrict__ st, co
 // (code/comp3.f:677-681,735-738,765-771).
 template <int TC>
 __device__ __forceinline__ void fz_reduce_column(const SegTable *__restrict__ st, const RtConst &K, const FzBuf &bf,
-                                                 int j, int max_nl, size_t stride, double *ws, int lane) {
-    const size_t row = (size_t)2 * max_nl;
+                                                 int j, int nv, int max_nl, size_t stride, double *ws, int lane) {
     double *fzf = ws;
     double *fmv = fzf + 12, *fmi = fmv + (D_MAXNL + 2), *misc = fmi + (D_MAXNL + 2);
     double *wa = misc + 4, *wb = wa + NSYS_V, *we = wb + NSYS_V;
@@ -211,7 +210,7 @@ __device__ __forceinline__ void fz_reduce_column(const SegTable *__restrict__ st
                     wa[nrow + lane] = a;
                     wb[nrow + lane] = b;
                     we[nrow + lane] = e;
-                    rpos[nrow + lane] = vis ? li : TC * NSYS_V + li;
+                    rpos[nrow + lane] = vis ? li : nv + li;   // row = solve order
                 }
                 nrow += gn;
             }
@@ -229,15 +228,15 @@ __device__ __forceinline__ void fz_reduce_column(const SegTable *__restrict__ st
                     up[q] = dn[q] = t0[q] = t1[q] = 0.0;
                     if (f0 + q < nrow) {
                         const size_t rr = (size_t)rpos[f0 + q];
-                        const double *pr = bf.fl + rr * row;
+                        const double *pr = bf.fl + row_base(rr, max_nl);
                         if (lv) {
-                            up[q] = pr[l - 1];
-                            dn[q] = pr[max_nl + l - 1];
+                            up[q] = pr[(size_t)(l - 1) * ROW_BLK];
+                            dn[q] = pr[(size_t)(max_nl + l - 1) * ROW_BLK];
                         }
                         if (r == 0) {
-                            const double *skp = bf.sc + rr * 4;
-                            t0[q] = vis ? skp[0] - skp[1] : skp[0];
-                            t1[q] = skp[2];
+                            const double *skp = bf.sc + sc_base(rr);
+                            t0[q] = vis ? skp[0] - skp[ROW_BLK] : skp[0];
+                            t1[q] = skp[2 * ROW_BLK];
                         }
                     }
                 }
@@ -337,7 +336,7 @@ rt_fused(const SegTable *__restrict__ st, int ncols, int max_nl, unsigned char *
         FzBuf r;
         r.blocks = scratch + (size_t)blockIdx.x * cta_bytes + (size_t)b * half;
         r.fl = reinterpret_cast<double *>(r.blocks + (size_t)TC * stride);
-        r.sc = r.fl + (size_t)TC * NSYS * row;
+        r.sc = r.fl + row_slots((size_t)TC * NSYS) * row;
         r.list = lists + (size_t)b * TC * NSYS;
         const long long g0 = (long long)tile * TC;
         r.g0 = g0 < total ? (int)g0 : 0;
@@ -378,8 +377,15 @@ rt_fused(const SegTable *__restrict__ st, int ncols, int max_nl, unsigned char *
                 s_cnt[nxt][0] = s_cnt[nxt][1] = 0;
                 if (bn.ng > 0) s_claim = (int)atomicAdd(tile_ctr, 1u);
             }
-            for (int i = atomicAdd(&s_solve, 1); i < nv + ni; i = atomicAdd(&s_solve, 1))
-                fz_solve_one<F32, TC>(st, K, kv, ki, kvf, bc, i, nv, max_nl, stride, w);
+            // a warp takes 32 consecutive systems at a time
+            for (;;) {
+                int b0 = 0;
+                if (lane == 0) b0 = atomicAdd(&s_solve, 32);
+                b0 = __shfl_sync(0xffffffffu, b0, 0);
+                if (b0 >= nv + ni) break;
+                if (b0 + lane < nv + ni)
+                    fz_solve_one<F32, TC>(st, K, kv, ki, kvf, bc, b0 + lane, nv, max_nl, stride, w);
+            }
             __syncwarp();
             for (int it = fz_warp_item(&s_stage, lane); it < bn.ng; it = fz_warp_item(&s_stage, lane))
                 fz_stage_column(st, K, planck, bn, it, max_nl, stride, status, lane);
@@ -390,7 +396,7 @@ rt_fused(const SegTable *__restrict__ st, int ncols, int max_nl, unsigned char *
             const int nred = bc.ng, nitems = nred + bn.ng * SCREEN_GROUPS;
             for (int it = fz_warp_item(&s_item, lane); it < nitems; it = fz_warp_item(&s_item, lane)) {
                 if (it < nred)
-                    fz_reduce_column<TC>(st, K, bc, it, max_nl, stride, ws, lane);
+                    fz_reduce_column<TC>(st, K, bc, it, nv, max_nl, stride, ws, lane);
                 else
                     fz_screen_item<F32, TC>(st, K, kv, ki, kvf, bn, it - nred, max_nl, stride, w, nsolved,
                                             s_cnt[nxt], lane);
