@@ -513,10 +513,12 @@ size_t reduce_smem_bytes(int max_nl, int rb) {
     (void)rb;
     return (size_t)RED_WARPS * red_warp_bytes();
 }
-// Systems whose loads the reduce issues before it sums them, by default.
+// Systems whose loads the reduce issues before it sums them, by default
+// (measured on the 64,800-column call: 4 -> 8 saves 0.07 ms; 16 needs 182
+// registers and is slower).
 int reduce_rows_per_chunk(int max_nl) {
     (void)max_nl;
-    return 4;
+    return 8;
 }
 // The reduce kernel of a launch: one level per lane up to NL = 32, and RB
 // in {1, 2, 4, 8} (other values round down).
