@@ -272,7 +272,7 @@ typedef struct mgcm_rt_tune {
     int chunk_cols;        /* columns per pipeline pass (fused form: columns per tile) */
     int solve_ctas_per_sm; /* solver CTAs per SM (0 = as many as fit; fused form: CTAs per SM
                               the register budget allows) */
-    int reduce_rows;       /* kept-system rows per TMA chunk of the reduce */
+    int reduce_rows;       /* kept systems whose loads a reduce lane issues before summing */
     int candidates;        /* launch shapes timed by the autotuner */
     int tuning_cols;       /* columns of the tuning sample */
     double default_ms;     /* built-in shape on the sample */
@@ -308,14 +308,6 @@ int mgcm_rt_dsolflux(mgcm_rt_handle *h, int ncol, int device_ptrs, const double 
  * Allocates a temporary staging buffer. */
 int mgcm_rt_debug_bins(mgcm_rt_handle *h, const mgcm_rt_batch_in *in, int *mt, int *mp, int *nh2o,
                        int *nplanck, double *wratio, double *lcoef);
-
-/* Self-check of the device waits (no counterpart in the reference): runs a
- * kernel whose wait can never be satisfied -- an mbarrier armed for bytes no
- * copy delivers -- through the same bounded wait the kernels use, and
- * returns MGCM_RT_OK when that wait gave up (about a second, *seconds if not
- * NULL) and reported it in the status word, MGCM_RT_ECUDA otherwise.  No
- * fault and no hang: the kernel returns normally and the handle stays usable. */
-int mgcm_rt_check_wait_bound(mgcm_rt_handle *h, double *seconds);
 
 int mgcm_rt_get_stats(mgcm_rt_handle *h, mgcm_rt_stats *st);
 

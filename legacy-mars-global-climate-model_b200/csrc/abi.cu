@@ -29,7 +29,6 @@
 #include "rt_aerosol.cuh"
 #include "rt_prep.cuh"
 #include "rt_column.cuh"
-#include "rt_tma.cuh"
 #include "tables.h"
 #include <nvtx3/nvToolsExt.h>
 
@@ -105,7 +104,6 @@ __global__ void rt_fused(const SegTable *__restrict__ st, int ncols, int max_nl,
                          uint32_t *status, unsigned long long *nsys);
 size_t fused_smem(int warps, int tc);
 size_t fused_scratch_per_cta(int tc, int max_nl, size_t stride);
-__global__ void rt_wait_probe(uint32_t *status);
 __global__ void rt_bins_decode(const SegTable *__restrict__ st, int ncol, int max_nl,
                                const unsigned char *__restrict__ blocks, size_t stride,
                                uint32_t *status, int *__restrict__ mt, int *__restrict__ mp,
@@ -790,7 +788,6 @@ int launch_all(mgcm_rt_handle *h, Slot &sl, cudaStream_t st, int total, int max_
 }
 
 int status_to_code(uint32_t st) {
-    if (st & ST_TMA_TIMEOUT) return MGCM_RT_ECUDA;   // a bounded device wait ran out
     if (st & ST_NONFINITE) return MGCM_RT_ENONFINITE;
     if (st & (ST_TEMP | ST_PLANCK_RANGE)) return MGCM_RT_ETEMP;
     if (st & ST_BADL) return MGCM_RT_ELAYERS;
@@ -1814,31 +1811,6 @@ int mgcm_rt_debug_bins(mgcm_rt_handle *h, const mgcm_rt_batch_in *in, int *mt, i
     } while (0);
     cudaFree(blocks);
     return rc;
-}
-
-int mgcm_rt_check_wait_bound(mgcm_rt_handle *h, double *seconds) {
-    if (!h) return MGCM_RT_EINVAL;
-    std::lock_guard<std::mutex> lk(h->mu);
-    if (cudaSetDevice(h->device) != cudaSuccess) return MGCM_RT_ECUDA;
-    if (int rc = finish_pending(h)) return rc;
-    Slot &sl = *h->slots[0];
-    cudaStream_t st = sync_stream(h);
-    CK(cudaMemsetAsync(sl.d_status, 0, 256, st));
-    CK(cudaEventRecord(sl.ev0, st));
-    rt_wait_probe<<<1, 32, 0, st>>>(sl.d_status);
-    CK(cudaGetLastError());
-    CK(cudaEventRecord(sl.ev1, st));
-    CK(cudaMemcpyAsync(sl.h_status, sl.d_status, 4, cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    float ms = 0.f;
-    cudaEventElapsedTime(&ms, sl.ev0, sl.ev1);
-    if (seconds) *seconds = ms * 1e-3;
-    const bool gave_up = (*sl.h_status & ST_TMA_TIMEOUT) != 0;
-    // leave the slot's status clean for the next call
-    CK(cudaMemsetAsync(sl.d_status, 0, 256, st));
-    CK(cudaStreamSynchronize(st));
-    *sl.h_status = 0;
-    return gave_up ? MGCM_RT_OK : MGCM_RT_ECUDA;
 }
 
 int mgcm_rt_run_state(mgcm_rt_handle *h, const mgcm_rt_batch_state *in, mgcm_rt_batch_out *out) {

@@ -28,7 +28,6 @@
 // the CPU oracle uses too, so host and device agree bit-for-bit.
 #include "rt_fp64_sys.cuh"
 #include "rt_quad.cuh"
-#include "rt_tma.cuh"
 #include "../../include/mgcm_rt_math.h"
 
 namespace mgcm {
@@ -556,18 +555,6 @@ __global__ void rt_dsolflux_kernel(int ncol, const double *__restrict__ sol,
     dnvflux[c] = dndiffv[c] + ds;
 }
 
-// Check of the bounded device waits: an mbarrier armed for 16 bytes that no
-// copy will deliver, waited on with the same bounded wait the reduce kernel
-// uses (rt_tma.cuh): it gives up after about a second and sets
-// ST_TMA_TIMEOUT in the status word, and the kernel returns normally.
-__global__ void rt_wait_probe(uint32_t *status) {
-    __shared__ __align__(8) uint64_t bar;
-    if (threadIdx.x == 0) {
-        mbar_init(&bar, 1);
-        mbar_arrive_expect_tx(&bar, 16);
-        mbar_wait(&bar, 0, status);
-    }
-}
 
 // Integer bins as the pipeline uses them, for the bit-exact check of
 // tpindex (code/tpindex.f90:72-134) and of the Planck index INT(T*10-499)

@@ -122,7 +122,6 @@ def lib():
         L.mgcm_rt_get_request_info.argtypes = [C.c_void_p, C.c_longlong, C.POINTER(RequestInfo)]
         L.mgcm_rt_dsolflux.argtypes = [C.c_void_p, C.c_int, C.c_int] + [C.c_void_p] * 5
         L.mgcm_rt_debug_bins.argtypes = [C.c_void_p, C.POINTER(BatchIn)] + [C.c_void_p] * 6
-        L.mgcm_rt_check_wait_bound.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
         L.mgcm_rt_enqueue.argtypes = [C.c_void_p, C.POINTER(BatchIn), C.POINTER(BatchOut)]
         L.mgcm_rt_sync.argtypes = [C.c_void_p]
         L.mgcm_rt_set_stream.argtypes = [C.c_void_p, C.c_void_p]
@@ -481,15 +480,6 @@ class Radiation:
         if rc != 0:
             raise RTError(rc, "mgcm_rt_debug_bins")
         return out
-
-    def check_wait_bound(self) -> float:
-        """Runs the bounded-wait self-check; returns the seconds the wait took
-        to give up (raises if it did not report)."""
-        sec = C.c_double(0.0)
-        rc = lib().mgcm_rt_check_wait_bound(self._h, C.byref(sec))
-        if rc != 0:
-            raise RTError(rc, "mgcm_rt_check_wait_bound")
-        return sec.value
 
     def stats(self) -> dict:
         s = Stats()
