@@ -85,7 +85,8 @@ def test_graph_fused_persistent_kernel(data_dir, otables, precision):
         try:
             info = g.info()
             assert info["kernels"] == 1, info
-            assert info["candidates"] >= 2 and info["threads_per_cta"] in (128, 256), info
+            # the tuner's pick among the fused launch shapes (128 to 512 threads)
+            assert info["candidates"] >= 2 and info["threads_per_cta"] in (128, 256, 320, 384, 512), info
             for _ in range(2):
                 g.launch()
                 torch.cuda.synchronize()
