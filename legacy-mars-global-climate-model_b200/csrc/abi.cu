@@ -321,6 +321,7 @@ struct mgcm_rt_handle {
     cudaEvent_t fork = nullptr, join0 = nullptr, join1 = nullptr;
     bool pending = false;
     long long pending_cols = 0;
+    int pending_parts = 1;                          // slots a pending device call runs on
     mgcm_rt_stats stats{};
     size_t budget = 0, used = 0;
     std::mutex mem_mu;
@@ -864,71 +865,119 @@ int issue_job(mgcm_rt_handle *h, Slot &sl, cudaStream_t st, const mgcm_rt_batch_
     return MGCM_RT_OK;
 }
 
-// Synchronous batch of device-pointer segments on slot 0 (async: leave pending).
-int run_device(mgcm_rt_handle *h, int nbatch, const mgcm_rt_batch_in *in, mgcm_rt_batch_out *out,
-               bool async) {
-    Slot &sl = *h->slots[0];
-    cudaStream_t st = sync_stream(h);
-    SegTable &tab = *sl.h_segs;
+// Device-pointer batches.  From 2 SPLIT_COLS columns on, the columns are
+// split in two halves that run concurrently on the two synchronous slots --
+// the first on the caller's stream, the second on slot 1's stream, forked
+// from and joined back into it -- so two halves' kernels share the SMs,
+// which these latency-bound kernels use better than one call's kernels
+// (two 32,400-column calls together: 12.06 ms, one 64,800-column call:
+// 12.66 ms).  The fused form, a persistent kernel that fills the GPU by
+// itself, runs unsplit.
+constexpr int SPLIT_COLS = 16384;
+
+// Segment table of the global columns [b0, b1) of the batches, every
+// per-column pointer shifted to the segment's first column in the range;
+// returns the table's columns.
+int table_of_range(SegTable &tab, int nbatch, const mgcm_rt_batch_in *in, const mgcm_rt_batch_out *out,
+                   int b0, int b1, int &max_nl) {
     tab.nseg = 0;
-    int total = 0, max_nl = 1;
+    int gcol = 0, pc = 0;
     for (int b = 0; b < nbatch; ++b) {
         const Sizes z = sizes_of(in[b]);
         if (z.ncol == 0) continue;
+        const int lo = std::max(b0, gcol), hi = std::min(b1, gcol + (int)z.ncol);
+        if (lo < hi) {
+            SegDev sd{};
+            sd.ncol = hi - lo;
+            sd.L = z.L;
+            sd.col0 = pc;
+            sd.ptrop = in[b].ptrop;
+            fill_direct(sd, in[b], out[b]);
+            for (auto &a : arrays_of(in[b], out[b], z, sd))
+                *a.seg_field = const_cast<double *>(a.src ? a.src : a.dst) + (size_t)(lo - gcol) * a.per_col;
+            sd.sigma = in[b].sigma;
+            sd.sol = in[b].sol;
+            tab.seg[tab.nseg++] = sd;
+            max_nl = std::max(max_nl, z.nl);
+            pc += hi - lo;
+        }
+        gcol += (int)z.ncol;
+    }
+    tab.total_cols = pc;
+    return pc;
+}
+
+int finish_pending(mgcm_rt_handle *h);
+
+// Synchronous batch of device-pointer segments (async: leave it pending).
+int run_device(mgcm_rt_handle *h, int nbatch, const mgcm_rt_batch_in *in, mgcm_rt_batch_out *out,
+               bool async) {
+    int total = 0;
+    for (int b = 0; b < nbatch; ++b) {
+        const Sizes z = sizes_of(in[b]);
         if ((long long)total + (long long)z.ncol > 0x7fffff) return MGCM_RT_EINVAL;
-        SegDev sd{};
-        sd.ncol = (int)z.ncol;
-        sd.L = z.L;
-        sd.col0 = total;
-        sd.ptrop = in[b].ptrop;
-        fill_direct(sd, in[b], out[b]);
-        sd.sigma = in[b].sigma;
-        sd.sol = in[b].sol;
-        tab.seg[tab.nseg++] = sd;
-        max_nl = std::max(max_nl, z.nl);
         total += (int)z.ncol;
     }
     if (total == 0) return MGCM_RT_OK;
-    tab.total_cols = total;
+    cudaStream_t st = sync_stream(h);
+    Slot &s0 = *h->slots[0];
     if (!h->user_stream) {
-        if (const int rc = after_legacy_stream(sl, st)) return rc;
+        if (const int rc = after_legacy_stream(s0, st)) return rc;
     }
-    CK(cudaMemcpyAsync(sl.d_segs, sl.h_segs, sizeof(SegTable), cudaMemcpyHostToDevice, st));
-    // pipeline chunk: bounded by a quarter of the budget
-    const size_t per_col = pipe_bytes_per_col(max_nl);
-    const int chunk = (int)std::max<size_t>(1, std::min<size_t>(total, (h->budget / 4) / per_col));
-    int rc = launch_all(h, sl, st, total, max_nl, chunk);
-    if (rc) return rc;
-    rc = post_status(sl, st);
-    if (rc) return rc;
+    const int nparts = (!h->fused && total >= 2 * SPLIT_COLS) ? 2 : 1;
+    if (nparts == 2) {
+        CK(cudaEventRecord(h->fork, st));
+        CK(cudaStreamWaitEvent(h->slots[1]->stream, h->fork, 0));
+    }
+    for (int p = 0; p < nparts; ++p) {
+        Slot &sl = *h->slots[p];
+        cudaStream_t ps = p == 0 ? st : sl.stream;
+        const int b0 = (int)((long long)total * p / nparts), b1 = (int)((long long)total * (p + 1) / nparts);
+        int max_nl = 1;
+        const int n = table_of_range(*sl.h_segs, nbatch, in, out, b0, b1, max_nl);
+        CK(cudaMemcpyAsync(sl.d_segs, sl.h_segs, sizeof(SegTable), cudaMemcpyHostToDevice, ps));
+        // pipeline chunk: bounded by a quarter of the budget
+        const size_t per_col = pipe_bytes_per_col(max_nl);
+        const int chunk = (int)std::max<size_t>(1, std::min<size_t>(n, (h->budget / 4) / per_col));
+        int rc = launch_all(h, sl, ps, n, max_nl, chunk);
+        if (rc) return rc;
+        rc = post_status(sl, ps);
+        if (rc) return rc;
+    }
+    if (nparts == 2) {
+        CK(cudaEventRecord(h->join1, h->slots[1]->stream));
+        CK(cudaStreamWaitEvent(st, h->join1, 0));
+        CK(cudaEventRecord(s0.ev1, st));   // the call ends when both halves have
+    }
     h->pending = true;
     h->pending_cols = total;
+    h->pending_parts = nparts;
     if (async) return MGCM_RT_OK;
-    CK(cudaStreamSynchronize(st));
-    h->pending = false;
-    float ms = 0.f;
-    cudaEventElapsedTime(&ms, sl.ev0, sl.ev1);
-    h->stats.gpu_ms = ms;
-    h->stats.columns = total;
-    h->stats.systems = (long long)*sl.h_nsys;
-    h->stats.status = (int)*sl.h_status;
-    h->stats.kernels = sl.kernels;
-    return status_to_code(*sl.h_status);
+    return finish_pending(h);
 }
 
 int finish_pending(mgcm_rt_handle *h) {
     if (!h->pending) return MGCM_RT_OK;
-    Slot &sl = *h->slots[0];
+    Slot &s0 = *h->slots[0];
     CK(cudaStreamSynchronize(sync_stream(h)));
     h->pending = false;
     float ms = 0.f;
-    cudaEventElapsedTime(&ms, sl.ev0, sl.ev1);
+    cudaEventElapsedTime(&ms, s0.ev0, s0.ev1);
+    uint32_t stw = *s0.h_status;
+    unsigned long long nsys = *s0.h_nsys;
+    int nk = s0.kernels;
+    if (h->pending_parts == 2) {
+        const Slot &s1 = *h->slots[1];
+        stw |= *s1.h_status;
+        nsys += *s1.h_nsys;
+        nk += s1.kernels;
+    }
     h->stats.gpu_ms = ms;
     h->stats.columns = h->pending_cols;
-    h->stats.systems = (long long)*sl.h_nsys;
-    h->stats.status = (int)*sl.h_status;
-    h->stats.kernels = sl.kernels;
-    return status_to_code(*sl.h_status);
+    h->stats.systems = (long long)nsys;
+    h->stats.status = (int)stw;
+    h->stats.kernels = nk;
+    return status_to_code(stw);
 }
 
 // Column ranges (ends) of a synchronous host-buffer call over n columns: jobs
