@@ -126,6 +126,9 @@ struct NvtxRange {
 };
 
 constexpr int BLOCK = 224;
+// Slots of the synchronous calls: host-buffer jobs alternate between the
+// first two; a device-pointer call runs up to all of them at once.
+constexpr int SYNC_SLOTS = 4;
 
 // On-chip solve kernels by family and threads per CTA (rt_onchip.cu).
 using OcKernel = void (*)(const SegTable *__restrict__, int, int, unsigned char *__restrict__, size_t,
@@ -316,7 +319,7 @@ struct mgcm_rt_handle {
     AeroConst aero{};         // aerosol optics constants (mgcm_rt_run_tracers)
     double *d_mie = nullptr;  // Mie tables on the device; null when the files were absent
     std::mutex mu;                                  // serialises the synchronous API
-    std::vector<std::unique_ptr<Slot>> slots;       // [0], [1]: synchronous calls
+    std::vector<std::unique_ptr<Slot>> slots;       // SYNC_SLOTS synchronous slots
     cudaStream_t user_stream = nullptr;             // mgcm_rt_set_stream
     cudaEvent_t fork = nullptr, join0 = nullptr, join1 = nullptr;
     bool pending = false;
@@ -865,15 +868,15 @@ int issue_job(mgcm_rt_handle *h, Slot &sl, cudaStream_t st, const mgcm_rt_batch_
     return MGCM_RT_OK;
 }
 
-// Device-pointer batches.  From 2 SPLIT_COLS columns on, the columns are
-// split in two halves that run concurrently on the two synchronous slots --
-// the first on the caller's stream, the second on slot 1's stream, forked
-// from and joined back into it -- so two halves' kernels share the SMs,
-// which these latency-bound kernels use better than one call's kernels
-// (two 32,400-column calls together: 12.06 ms, one 64,800-column call:
-// 12.66 ms).  The fused form, a persistent kernel that fills the GPU by
-// itself, runs unsplit.
-constexpr int SPLIT_COLS = 16384;
+// Device-pointer batches.  The columns are split into up to SYNC_SLOTS parts
+// of at least SPLIT_COLS columns that run concurrently on the synchronous
+// slots -- the first on the caller's stream, the others on their slots'
+// streams, forked from and joined back into it -- so the parts' kernels share
+// the SMs, which these latency-bound kernels use better than one call's
+// kernels (64,800 columns: 12.66 ms in one call; as 2 / 3 / 4 concurrent
+// calls 12.2 / 12.0 / 11.9 ms).  The fused form, a persistent kernel that
+// fills the GPU by itself, runs unsplit.
+constexpr int SPLIT_COLS = 12288;
 
 // Segment table of the global columns [b0, b1) of the batches, every
 // per-column pointer shifted to the segment's first column in the range;
@@ -924,10 +927,10 @@ int run_device(mgcm_rt_handle *h, int nbatch, const mgcm_rt_batch_in *in, mgcm_r
     if (!h->user_stream) {
         if (const int rc = after_legacy_stream(s0, st)) return rc;
     }
-    const int nparts = (!h->fused && total >= 2 * SPLIT_COLS) ? 2 : 1;
-    if (nparts == 2) {
+    const int nparts = h->fused ? 1 : std::max(1, std::min(SYNC_SLOTS, total / SPLIT_COLS));
+    if (nparts > 1) {
         CK(cudaEventRecord(h->fork, st));
-        CK(cudaStreamWaitEvent(h->slots[1]->stream, h->fork, 0));
+        for (int p = 1; p < nparts; ++p) CK(cudaStreamWaitEvent(h->slots[p]->stream, h->fork, 0));
     }
     for (int p = 0; p < nparts; ++p) {
         Slot &sl = *h->slots[p];
@@ -936,18 +939,22 @@ int run_device(mgcm_rt_handle *h, int nbatch, const mgcm_rt_batch_in *in, mgcm_r
         int max_nl = 1;
         const int n = table_of_range(*sl.h_segs, nbatch, in, out, b0, b1, max_nl);
         CK(cudaMemcpyAsync(sl.d_segs, sl.h_segs, sizeof(SegTable), cudaMemcpyHostToDevice, ps));
-        // pipeline chunk: bounded by a quarter of the budget
+        // pipeline chunk: the parts' scratch together within half the budget
+        // (one part: a quarter)
         const size_t per_col = pipe_bytes_per_col(max_nl);
-        const int chunk = (int)std::max<size_t>(1, std::min<size_t>(n, (h->budget / 4) / per_col));
+        const size_t share = h->budget / (nparts > 1 ? 2 * nparts : 4);
+        const int chunk = (int)std::max<size_t>(1, std::min<size_t>(n, share / per_col));
         int rc = launch_all(h, sl, ps, n, max_nl, chunk);
         if (rc) return rc;
         rc = post_status(sl, ps);
         if (rc) return rc;
     }
-    if (nparts == 2) {
-        CK(cudaEventRecord(h->join1, h->slots[1]->stream));
-        CK(cudaStreamWaitEvent(st, h->join1, 0));
-        CK(cudaEventRecord(s0.ev1, st));   // the call ends when both halves have
+    if (nparts > 1) {
+        for (int p = 1; p < nparts; ++p) {
+            CK(cudaEventRecord(h->slots[p]->done, h->slots[p]->stream));
+            CK(cudaStreamWaitEvent(st, h->slots[p]->done, 0));
+        }
+        CK(cudaEventRecord(s0.ev1, st));   // the call ends when every part has
     }
     h->pending = true;
     h->pending_cols = total;
@@ -966,11 +973,11 @@ int finish_pending(mgcm_rt_handle *h) {
     uint32_t stw = *s0.h_status;
     unsigned long long nsys = *s0.h_nsys;
     int nk = s0.kernels;
-    if (h->pending_parts == 2) {
-        const Slot &s1 = *h->slots[1];
-        stw |= *s1.h_status;
-        nsys += *s1.h_nsys;
-        nk += s1.kernels;
+    for (int p = 1; p < h->pending_parts; ++p) {
+        const Slot &sp = *h->slots[p];
+        stw |= *sp.h_status;
+        nsys += *sp.h_nsys;
+        nk += sp.kernels;
     }
     h->stats.gpu_ms = ms;
     h->stats.columns = h->pending_cols;
@@ -1608,7 +1615,7 @@ mgcm_rt_handle *mgcm_rt_create(const mgcm_rt_config *cfg, const char *data_dir, 
     h->onchip = cfg->solver == MGCM_RT_SOLVER_ONCHIP;
     h->num_sms = prop.multiProcessorCount;
     auto fail = [&](int code) { mgcm_rt_destroy(h.release()); *status = code; return nullptr; };
-    for (int i = 0; i < 2; ++i) {
+    for (int i = 0; i < SYNC_SLOTS; ++i) {
         h->slots.push_back(std::make_unique<Slot>());
         if (slot_init(*h->slots.back())) return fail(MGCM_RT_ECUDA);
     }
