@@ -1981,15 +1981,22 @@ int mgcm_rt_wait(mgcm_rt_handle *h, long long ticket, double timeout_s) {
 }
 
 // ---------------------------------------------------------------------------
-// Captured uneven batches: segment table built once, launch shape autotuned,
-// the pipeline captured into a CUDA graph on the graph's own slot.
+// Captured uneven batches: segment tables built once, launch shape
+// autotuned, the pipeline captured into a CUDA graph.  As for device-pointer
+// calls, the columns are split into up to SYNC_SLOTS concurrent parts (part 0
+// on the graph's slot, the others on their own slots, forked and joined
+// inside the graph); the fused form runs as one part.
 struct mgcm_rt_graph {
     mgcm_rt_handle *h = nullptr;
-    Slot slot;
+    Slot slot;                        // part 0
+    Slot parts[SYNC_SLOTS - 1];       // parts 1 .. nparts-1
+    int nparts = 1, ncols[SYNC_SLOTS] = {}, part_nl[SYNC_SLOTS] = {};
+    cudaEvent_t fork = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     int total = 0, max_nl = 1, max_chunk = 1;
     mgcm_rt_tune info{};
+    Slot &part(int p) { return p == 0 ? slot : parts[p - 1]; }
 };
 
 namespace {
@@ -2005,7 +2012,7 @@ int time_shape(mgcm_rt_graph *g, const Tune &t, int cols, float &ms) {
     for (int rep = 0; rep < 2; ++rep) {
         CK(cudaMemsetAsync(sl.d_status, 0, 256, st));
         CK(cudaEventRecord(sl.ev0, st));
-        int rc = launch_body(h, sl, st, cols, g->max_nl, nk, g->max_chunk);
+        int rc = launch_body(h, sl, st, cols, g->part_nl[0], nk, g->max_chunk);
         if (rc) return rc;
         CK(cudaEventRecord(sl.ev1, st));
         CK(cudaStreamSynchronize(st));
@@ -2021,7 +2028,9 @@ void graph_free(mgcm_rt_graph *g) {
     if (!g) return;
     if (g->exec) cudaGraphExecDestroy(g->exec);
     if (g->graph) cudaGraphDestroy(g->graph);
-    if (g->h) slot_free(g->h, g->slot);
+    if (g->fork) cudaEventDestroy(g->fork);
+    if (g->h)
+        for (int p = 0; p < g->nparts; ++p) slot_free(g->h, g->part(p));
     delete g;
 }
 
@@ -2043,36 +2052,46 @@ int mgcm_rt_graph_create(mgcm_rt_handle *h, int nbatch, const mgcm_rt_batch_in *
     mgcm_rt_graph *g = new mgcm_rt_graph;
     g->h = h;
     auto fail = [&](int code) { graph_free(g); return code; };
-    if (slot_init(g->slot)) return fail(MGCM_RT_ECUDA);
-    Slot &sl = g->slot;
-    SegTable &tab = *sl.h_segs;
-    tab.nseg = 0;
     int total = 0, max_nl = 1;
     for (int b = 0; b < nbatch; ++b) {
         const Sizes z = sizes_of(in[b]);
-        if (z.ncol == 0) continue;
-        if ((long long)total + (long long)z.ncol > 0x7fffff) return fail(MGCM_RT_EINVAL);
-        SegDev sd{};
-        sd.ncol = (int)z.ncol;
-        sd.L = z.L;
-        sd.col0 = total;
-        sd.ptrop = in[b].ptrop;
-        fill_direct(sd, in[b], out[b]);
-        sd.sigma = in[b].sigma;
-        sd.sol = in[b].sol;
-        tab.seg[tab.nseg++] = sd;
-        max_nl = std::max(max_nl, z.nl);
+        if ((long long)total + (long long)z.ncol > 0x7fffff) {
+            delete g;
+            return MGCM_RT_EINVAL;
+        }
         total += (int)z.ncol;
+        if (z.ncol) max_nl = std::max(max_nl, z.nl);
     }
-    if (total == 0) return fail(MGCM_RT_EINVAL);
-    tab.total_cols = total;
-    if (cudaMemcpyAsync(sl.d_segs, sl.h_segs, sizeof(SegTable), cudaMemcpyHostToDevice, sl.stream) ||
-        cudaStreamSynchronize(sl.stream))
-        return fail(MGCM_RT_ECUDA);
+    if (total == 0) {
+        delete g;
+        return MGCM_RT_EINVAL;
+    }
+    g->nparts = h->fused ? 1 : std::max(1, std::min(SYNC_SLOTS, total / SPLIT_COLS));
+    for (int p = 0; p < g->nparts; ++p)
+        if (slot_init(g->part(p))) {
+            g->nparts = p + 1;   // slot_free the ones begun
+            return fail(MGCM_RT_ECUDA);
+        }
+    if (cudaEventCreateWithFlags(&g->fork, cudaEventDisableTiming)) return fail(MGCM_RT_ECUDA);
+    for (int p = 0; p < g->nparts; ++p) {
+        Slot &ps = g->part(p);
+        const int b0 = (int)((long long)total * p / g->nparts), b1 = (int)((long long)total * (p + 1) / g->nparts);
+        int nl = 1;
+        g->ncols[p] = table_of_range(*ps.h_segs, nbatch, in, out, b0, b1, nl);
+        g->part_nl[p] = nl;
+        if (cudaMemcpyAsync(ps.d_segs, ps.h_segs, sizeof(SegTable), cudaMemcpyHostToDevice, ps.stream) ||
+            cudaStreamSynchronize(ps.stream))
+            return fail(MGCM_RT_ECUDA);
+    }
+    Slot &sl = g->slot;
     g->total = total;
     g->max_nl = max_nl;
+    // the parts' scratch together within a quarter of the budget, which the
+    // handle's own calls can use beside the graph's
     const size_t per_col = pipe_bytes_per_col(max_nl);
-    g->max_chunk = (int)std::max<size_t>(1, std::min<size_t>(total, (h->budget / 4) / per_col));
+    const size_t share = h->budget / (4 * g->nparts);
+    const int most = *std::max_element(g->ncols, g->ncols + g->nparts);
+    g->max_chunk = (int)std::max<size_t>(1, std::min<size_t>(most, share / per_col));
 
     // autotune: coordinate descent over chunk, solver CTAs per SM and reduce
     // rows per chunk, each shape timed (best of two) on the first columns
@@ -2080,7 +2099,7 @@ int mgcm_rt_graph_create(mgcm_rt_handle *h, int nbatch, const mgcm_rt_batch_in *
     // tuning sample: the first 131,072 columns for the pipeline; the whole
     // batch (up to 1M columns) for the fused kernel, whose best shape depends
     // on the mix of layer counts, which the first members need not represent
-    const int sample = h->fused ? std::min(total, 1 << 20) : std::min(total, 131072);
+    const int sample = h->fused ? std::min(g->ncols[0], 1 << 20) : std::min(g->ncols[0], 131072);
     float t_def = 0.f;
     int rc = time_shape(g, best, sample, t_def);
     if (rc) return fail(rc);
@@ -2132,19 +2151,39 @@ int mgcm_rt_graph_create(mgcm_rt_handle *h, int nbatch, const mgcm_rt_batch_in *
             if ((rc = consider(t))) return fail(rc);
         }
     }
-    sl.tune = best;
-    // one eager pass over every column with the chosen shape sizes the
-    // scratch for the capture (nothing may allocate while capturing)
-    float t_full = 0.f;
-    if ((rc = time_shape(g, best, total, t_full))) return fail(rc);
+    // one eager pass over every part's columns with the chosen shape sizes
+    // the scratch for the capture (nothing may allocate while capturing)
+    for (int p = 0; p < g->nparts; ++p) {
+        Slot &ps = g->part(p);
+        ps.tune = best;
+        int nk0 = 0;
+        if ((rc = launch_body(h, ps, ps.stream, g->ncols[p], g->part_nl[p], nk0, g->max_chunk))) return fail(rc);
+        if (cudaStreamSynchronize(ps.stream) != cudaSuccess) return fail(MGCM_RT_ECUDA);
+    }
 
     int nk = 0;
     cudaStream_t st = sl.stream;
     if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return fail(MGCM_RT_ECUDA);
     int crc = MGCM_RT_OK;
     if (cudaMemsetAsync(sl.d_status, 0, 256, st) != cudaSuccess) crc = MGCM_RT_ECUDA;
-    if (!crc) crc = launch_body(h, sl, st, total, max_nl, nk, g->max_chunk);
-    if (!crc) crc = post_status(sl, st);
+    if (!crc && g->nparts > 1 && cudaEventRecord(g->fork, st) != cudaSuccess) crc = MGCM_RT_ECUDA;
+    for (int p = 1; p < g->nparts && !crc; ++p) {
+        Slot &ps = g->part(p);
+        if (cudaStreamWaitEvent(ps.stream, g->fork, 0) != cudaSuccess ||
+            cudaMemsetAsync(ps.d_status, 0, 256, ps.stream) != cudaSuccess)
+            crc = MGCM_RT_ECUDA;
+    }
+    for (int p = 0; p < g->nparts && !crc; ++p) {
+        Slot &ps = g->part(p);
+        cudaStream_t pst = p == 0 ? st : ps.stream;
+        crc = launch_body(h, ps, pst, g->ncols[p], g->part_nl[p], nk, g->max_chunk);
+        if (!crc) crc = post_status(ps, pst);
+    }
+    for (int p = 1; p < g->nparts && !crc; ++p) {
+        Slot &ps = g->part(p);
+        if (cudaEventRecord(ps.done, ps.stream) != cudaSuccess || cudaStreamWaitEvent(st, ps.done, 0) != cudaSuccess)
+            crc = MGCM_RT_ECUDA;
+    }
     cudaGraph_t gr = nullptr;
     const cudaError_t ce = cudaStreamEndCapture(st, &gr);
     if (crc || ce != cudaSuccess || !gr) {
@@ -2184,7 +2223,9 @@ int mgcm_rt_graph_launch(mgcm_rt_graph *g, void *stream) {
 
 int mgcm_rt_graph_status(mgcm_rt_graph *g) {
     if (!g) return MGCM_RT_EINVAL;
-    return status_to_code(*g->slot.h_status);
+    uint32_t st = 0;
+    for (int p = 0; p < g->nparts; ++p) st |= *g->part(p).h_status;
+    return status_to_code(st);
 }
 
 int mgcm_rt_graph_info(const mgcm_rt_graph *g, mgcm_rt_tune *info) {
