@@ -126,9 +126,14 @@ struct NvtxRange {
 };
 
 constexpr int BLOCK = 224;
-// Slots of the synchronous calls: host-buffer jobs alternate between the
-// first two; a device-pointer call runs up to all of them at once.
+// Slots of the synchronous calls: host-buffer jobs rotate over the first
+// JOB_SLOTS; a device-pointer call runs up to all of them at once.
 constexpr int SYNC_SLOTS = 4;
+#ifndef MGCM_JOB_SLOTS
+#define MGCM_JOB_SLOTS 4
+#endif
+constexpr int JOB_SLOTS = MGCM_JOB_SLOTS;
+static_assert(JOB_SLOTS >= 1 && JOB_SLOTS <= SYNC_SLOTS, "job slots");
 
 // On-chip solve kernels by family and threads per CTA (rt_onchip.cu).
 using OcKernel = void (*)(const SegTable *__restrict__, int, int, unsigned char *__restrict__, size_t,
@@ -192,7 +197,10 @@ int tm_choice(bool vis, int nl) {
     }
     return -1;
 }
-constexpr int SYNC_JOB_COLS = 8192;     // columns per job of a synchronous host-buffer call (measured best of 2k-32k)
+#ifndef MGCM_SYNC_JOB_COLS
+#define MGCM_SYNC_JOB_COLS 8192
+#endif
+constexpr int SYNC_JOB_COLS = MGCM_SYNC_JOB_COLS;   // columns per job of a synchronous host-buffer call
 #ifndef MGCM_SYNC_RAMP
 #define MGCM_SYNC_RAMP 2048
 #endif
@@ -321,7 +329,7 @@ struct mgcm_rt_handle {
     std::mutex mu;                                  // serialises the synchronous API
     std::vector<std::unique_ptr<Slot>> slots;       // SYNC_SLOTS synchronous slots
     cudaStream_t user_stream = nullptr;             // mgcm_rt_set_stream
-    cudaEvent_t fork = nullptr, join0 = nullptr, join1 = nullptr;
+    cudaEvent_t fork = nullptr;
     bool pending = false;
     long long pending_cols = 0;
     int pending_parts = 1;                          // slots a pending device call runs on
@@ -1011,7 +1019,7 @@ std::vector<int> job_ends(int n, int max_job, int first) {
     return ends;
 }
 
-// Synchronous batch of host-pointer segments: jobs alternate between the two
+// Synchronous batch of host-pointer segments: jobs rotate over JOB_SLOTS
 // synchronous slots, forked from and joined back into the caller's stream.
 int run_host(mgcm_rt_handle *h, int nbatch, const mgcm_rt_batch_in *in, mgcm_rt_batch_out *out) {
     cudaStream_t ust = sync_stream(h);
@@ -1023,13 +1031,13 @@ int run_host(mgcm_rt_handle *h, int nbatch, const mgcm_rt_batch_in *in, mgcm_rt_
     uint32_t acc = 0;
     long long cols = 0, systems = 0;
     int nk = 0, k = 0;
-    bool used[2] = {false, false};
+    bool used[JOB_SLOTS] = {};
     for (int b = 0; b < nbatch; ++b) {
         const Sizes z = sizes_of(in[b]);
         int c0 = 0;
         for (const int c1 : job_ends((int)z.ncol, SYNC_JOB_COLS, SYNC_RAMP_COLS)) {
-            Slot &sl = *h->slots[k & 1];
-            if (used[k & 1]) {   // the slot's previous job must finish before its buffers are reused
+            Slot &sl = *h->slots[k % JOB_SLOTS];
+            if (used[k % JOB_SLOTS]) {   // the slot's previous job must finish before its buffers are reused
                 CK(cudaEventSynchronize(sl.done));
                 acc |= *sl.h_status;
                 systems += (long long)*sl.h_nsys;
@@ -1039,25 +1047,22 @@ int run_host(mgcm_rt_handle *h, int nbatch, const mgcm_rt_batch_in *in, mgcm_rt_
                 for (auto &s : h->slots) cudaStreamSynchronize(s->stream);
                 return rc;
             }
-            used[k & 1] = true;
+            used[k % JOB_SLOTS] = true;
             nk += sl.kernels;
             cols += c1 - c0;
             c0 = c1;
             ++k;
         }
     }
-    for (int i = 0; i < 2; ++i) {
+    for (int i = 0; i < JOB_SLOTS; ++i) {
         Slot &sl = *h->slots[i];
         if (used[i]) {
             CK(cudaEventSynchronize(sl.done));
             acc |= *sl.h_status;
             systems += (long long)*sl.h_nsys;
+            CK(cudaStreamWaitEvent(ust, sl.done, 0));
         }
     }
-    CK(cudaEventRecord(h->join0, h->slots[0]->stream));
-    CK(cudaEventRecord(h->join1, h->slots[1]->stream));
-    CK(cudaStreamWaitEvent(ust, h->join0, 0));
-    CK(cudaStreamWaitEvent(ust, h->join1, 0));
     float ms = 0.f;
     if (used[0]) cudaEventElapsedTime(&ms, h->slots[0]->ev0, h->slots[0]->ev1);
     h->stats.gpu_ms = ms;
@@ -1374,13 +1379,13 @@ int run_tracers(mgcm_rt_handle *h, const mgcm_rt_batch_tracers &in, mgcm_rt_batc
     uint32_t acc = 0;
     long long systems = 0;
     int nk = 0, k = 0;
-    bool used[2] = {false, false};
+    bool used[JOB_SLOTS] = {};
     const std::vector<int> ends = in.device_ptrs ? job_ends(in.ncol, 4 * SYNC_JOB_COLS, 0)
                                                  : job_ends(in.ncol, SYNC_JOB_COLS, SYNC_RAMP_COLS);
     int c0 = 0;
     for (const int c1 : ends) {
-        Slot &sl = *h->slots[k & 1];
-        if (used[k & 1]) {
+        Slot &sl = *h->slots[k % JOB_SLOTS];
+        if (used[k % JOB_SLOTS]) {
             CK(cudaEventSynchronize(sl.done));
             acc |= *sl.h_status;
             systems += (long long)*sl.h_nsys;
@@ -1390,23 +1395,20 @@ int run_tracers(mgcm_rt_handle *h, const mgcm_rt_batch_tracers &in, mgcm_rt_batc
             for (auto &s : h->slots) cudaStreamSynchronize(s->stream);
             return rc;
         }
-        used[k & 1] = true;
+        used[k % JOB_SLOTS] = true;
         nk += sl.kernels;
         c0 = c1;
         ++k;
     }
-    for (int i = 0; i < 2; ++i) {
+    for (int i = 0; i < JOB_SLOTS; ++i) {
         Slot &sl = *h->slots[i];
         if (used[i]) {
             CK(cudaEventSynchronize(sl.done));
             acc |= *sl.h_status;
             systems += (long long)*sl.h_nsys;
+            CK(cudaStreamWaitEvent(ust, sl.done, 0));
         }
     }
-    CK(cudaEventRecord(h->join0, h->slots[0]->stream));
-    CK(cudaEventRecord(h->join1, h->slots[1]->stream));
-    CK(cudaStreamWaitEvent(ust, h->join0, 0));
-    CK(cudaStreamWaitEvent(ust, h->join1, 0));
     float ms = 0.f;
     if (used[0]) cudaEventElapsedTime(&ms, h->slots[0]->ev0, h->slots[0]->ev1);
     h->stats.gpu_ms = ms;
@@ -1619,10 +1621,7 @@ mgcm_rt_handle *mgcm_rt_create(const mgcm_rt_config *cfg, const char *data_dir, 
         h->slots.push_back(std::make_unique<Slot>());
         if (slot_init(*h->slots.back())) return fail(MGCM_RT_ECUDA);
     }
-    if (cudaEventCreateWithFlags(&h->fork, cudaEventDisableTiming) ||
-        cudaEventCreateWithFlags(&h->join0, cudaEventDisableTiming) ||
-        cudaEventCreateWithFlags(&h->join1, cudaEventDisableTiming))
-        return fail(MGCM_RT_ECUDA);
+    if (cudaEventCreateWithFlags(&h->fork, cudaEventDisableTiming)) return fail(MGCM_RT_ECUDA);
     RtConst &K = h->K;
     std::memcpy(K.tauray, h->host.tauray, sizeof(K.tauray));
     std::memcpy(K.fzerov, h->host.fzerov, sizeof(K.fzerov));
@@ -1713,8 +1712,6 @@ void mgcm_rt_destroy(mgcm_rt_handle *h) {
     cudaFree(h->d_mie);
     cudaFree(h->d_planck);
     if (h->fork) cudaEventDestroy(h->fork);
-    if (h->join0) cudaEventDestroy(h->join0);
-    if (h->join1) cudaEventDestroy(h->join1);
     if (h->epoch) cudaEventDestroy(h->epoch);
     delete h;
 }
