@@ -80,7 +80,7 @@ typedef struct {
     int solver;           /* MGCM_RT_SOLVER_AUTO / _THREAD: one thread per (band, Gauss)
                              system; MGCM_RT_SOLVER_QUAD: four lanes per system with the
                              per-layer values in registers (L <= 51; same results) */
-    int max_queued_jobs;  /* serving: jobs (of <= 32,768 columns) accepted and not yet
+    int max_queued_jobs;  /* serving: jobs (of <= 16,384 columns) accepted and not yet
                              finished, at most; a submit beyond it returns MGCM_RT_EBUSY.
                              0 = 100,000 */
 } mgcm_rt_config;
@@ -168,7 +168,7 @@ int mgcm_rt_run_multi(mgcm_rt_handle *h, int nbatch, const mgcm_rt_batch_in *in,
                       mgcm_rt_batch_out *out);
 
 /* Serving: queue a batch (pointers must stay valid until collected), get a
- * ticket.  Requests are split into jobs of <= 32,768 columns and admitted
+ * ticket.  Requests are split into jobs of <= 16,384 columns and admitted
  * onto up to four serving slots as slots and HBM budget free up; a job that
  * does not fit the budget while others run waits for them (a job that does
  * not fit an idle device fails with MGCM_RT_ENOMEM).  MGCM_RT_EBUSY when the
@@ -192,7 +192,7 @@ int mgcm_rt_wait(mgcm_rt_handle *h, long long ticket, double timeout_s);
 typedef struct {
     int done;               /* 1 when every job has finished */
     int status;             /* request status so far (0 or a negative code) */
-    int jobs;               /* jobs of <= 32,768 columns the request was split into */
+    int jobs;               /* jobs of <= 16,384 columns the request was split into */
     int deferred;           /* admissions put back because the HBM budget was full */
     double submit_ms, done_ms;                 /* host */
     double device_begin_ms, device_end_ms;     /* device */

@@ -205,7 +205,10 @@ constexpr int SYNC_JOB_COLS = MGCM_SYNC_JOB_COLS;   // columns per job of a sync
 #define MGCM_SYNC_RAMP 2048
 #endif
 constexpr int SYNC_RAMP_COLS = MGCM_SYNC_RAMP;   // first (and last) job of a ramped host-buffer call
-constexpr int SERVE_JOB_COLS = 32768;   // columns per job of a served request
+#ifndef MGCM_SERVE_JOB_COLS
+#define MGCM_SERVE_JOB_COLS 16384
+#endif
+constexpr int SERVE_JOB_COLS = MGCM_SERVE_JOB_COLS;   // columns per job of a served request
 constexpr int SERVE_SLOTS = 4;          // serving slots at most
 
 // ---------------------------------------------------------------- validation

@@ -119,7 +119,7 @@ def test_hbm_budget_defers_admission_then_completes(data_dir):
     """With an HBM budget that holds one job's staging but not two, the
     second and third requests wait for the first (their admissions are put
     back, counted in `deferred`) and still complete with the right results."""
-    n = 30000
+    n = 12000   # one served job per request
     probe = abi.Radiation(data_dir, max_layers=24, precision=abi.FP64, validate=False)
     try:
         batches = [synth.make_batch(n, L=24, seed=80 + i, cloud=True) for i in range(3)]
@@ -152,14 +152,17 @@ def test_hbm_budget_defers_admission_then_completes(data_dir):
         rt.close()
 
 
+JOB = 16384   # columns per served job (the library's SERVE_JOB_COLS)
+
+
 def test_queue_full_is_ebusy(data_dir):
     rt = abi.Radiation(data_dir, max_layers=24, precision=abi.FP64, validate=False, max_queued_jobs=2)
     try:
-        big = synth.make_batch(3 * 32768, L=24, seed=90, cloud=True)   # 3 jobs: never fits
+        big = synth.make_batch(3 * JOB, L=24, seed=90, cloud=True)   # 3 jobs: never fits
         with pytest.raises(abi.RTError) as e:
             rt.submit(_device(big))
         assert e.value.code == -9
-        two = _device(synth.make_batch(2 * 32768, L=24, seed=91, cloud=True))   # 2 jobs: fills the queue
+        two = _device(synth.make_batch(2 * JOB, L=24, seed=91, cloud=True))   # 2 jobs: fills the queue
         one = _device(synth.make_batch(100, L=24, seed=92, cloud=True))
         t, out = rt.submit(two)
         with pytest.raises(abi.RTError) as e:
