@@ -943,22 +943,29 @@ int run_device(mgcm_rt_handle *h, int nbatch, const mgcm_rt_batch_in *in, mgcm_r
         CK(cudaEventRecord(h->fork, st));
         for (int p = 1; p < nparts; ++p) CK(cudaStreamWaitEvent(h->slots[p]->stream, h->fork, 0));
     }
+    // a part that fails to launch leaves the ones issued before it running on
+    // the caller's buffers and the slots' scratch: wait for them
+    auto drain = [&](int rc, int issued) {
+        cudaStreamSynchronize(st);
+        for (int q = 1; q <= issued && q < nparts; ++q) cudaStreamSynchronize(h->slots[q]->stream);
+        return rc;
+    };
     for (int p = 0; p < nparts; ++p) {
         Slot &sl = *h->slots[p];
         cudaStream_t ps = p == 0 ? st : sl.stream;
         const int b0 = (int)((long long)total * p / nparts), b1 = (int)((long long)total * (p + 1) / nparts);
         int max_nl = 1;
         const int n = table_of_range(*sl.h_segs, nbatch, in, out, b0, b1, max_nl);
-        CK(cudaMemcpyAsync(sl.d_segs, sl.h_segs, sizeof(SegTable), cudaMemcpyHostToDevice, ps));
+        if (cudaMemcpyAsync(sl.d_segs, sl.h_segs, sizeof(SegTable), cudaMemcpyHostToDevice, ps) != cudaSuccess)
+            return drain(MGCM_RT_ECUDA, p);
         // pipeline chunk: the parts' scratch together within half the budget
         // (one part: a quarter)
         const size_t per_col = pipe_bytes_per_col(max_nl);
         const size_t share = h->budget / (nparts > 1 ? 2 * nparts : 4);
         const int chunk = (int)std::max<size_t>(1, std::min<size_t>(n, share / per_col));
         int rc = launch_all(h, sl, ps, n, max_nl, chunk);
-        if (rc) return rc;
-        rc = post_status(sl, ps);
-        if (rc) return rc;
+        if (!rc) rc = post_status(sl, ps);
+        if (rc) return drain(rc, p);
     }
     if (nparts > 1) {
         for (int p = 1; p < nparts; ++p) {
