@@ -1,4 +1,5 @@
-"""The no-allocation entry point (mgcm_rt_run_noalloc) against the oracle.
+"""The no-allocation entry point (mgcm_rt_run_noalloc) against the oracle and
+against the allocating entry point (mgcm_rt_run) on the same inputs.
 
 mgcm_rt_run_noalloc serves callers that must not allocate device memory
 after start-up (a host whose device memory belongs to another allocator, a
@@ -50,6 +51,8 @@ def test_noalloc_matches_oracle_twice(data_dir, otables, ncol, L, cloud, seed):
     try:
         b = synth.make_batch(ncol, L=L, seed=seed, cloud=cloud)
         ref = oracle.run_batch(otables, b)
+        # the allocating entry point (mgcm_rt_run) on the same inputs
+        run_out = to_numpy(rt.run(_device(b)))
         for rep in range(2):
             bd = _device(b)    # fresh DETAU/CUMTAUV: they are in/out
             out = abi.alloc_outputs(ncol, L, device=torch.device("cuda", 0))
@@ -60,8 +63,11 @@ def test_noalloc_matches_oracle_twice(data_dir, otables, ncol, L, cloud, seed):
             assert rc == 0, abi.lib().mgcm_rt_strerror(rc)
             assert free1 == free0, f"call {rep}: device free memory changed by {free0 - free1} bytes"
             out["detau"], out["cumtauv"] = bd["detau"], bd["cumtauv"]
-            err = compare(b, to_numpy(out), ref, RTOL)
+            got = to_numpy(out)
+            err = compare(b, got, ref, RTOL)
             assert max(err.values()) <= RTOL, err
+            err = compare(b, got, run_out, RTOL)
+            assert max(err.values()) <= RTOL, ("against mgcm_rt_run", err)
     finally:
         rt.close()
 
