@@ -166,3 +166,61 @@ def test_bins_reject_host_pointers(data_dir):
         assert rc == -1
     finally:
         rt.close()
+
+
+def _beyond_grid_batch():
+    """Four columns whose TMID, PMID and QH2O lie beyond the ends of the
+    k-table grids (TREF 50..350 K, the 51 reference pressures, WREFH2O);
+    TPINDEX clamps them to the edge bins (code/tpindex.f90:72-134).  TLEV
+    stays inside the Planck table."""
+    b = synth.make_batch(4, L=24, seed=43, cloud=True, night_frac=0.0)
+    b["tmid"][0, 1:] = 5.0
+    b["tmid"][1, 1:] = 1000.0
+    b["tmid"][2, 1::2] = 49.0
+    b["tmid"][2, 2::2] = 351.0
+    b["pmid"][0, 1:] = 1.0e-10
+    b["pmid"][1, 1:] = 1.0e5
+    b["qh2o"][2, 1:] = 0.0
+    b["qh2o"][3, 1:] = 5.0
+    return b
+
+
+def test_bins_clamped_beyond_the_tables(data_dir, otables):
+    """The k-table indices the device forms stay inside the tables whatever
+    the state: MT in 1..6, MP in 1..50, NH2O in 1..10, and equal to the
+    oracle's.  They are bounded by construction (every search falls back to
+    an edge bin), so no gather can leave the table."""
+    rt = abi.Radiation(data_dir, max_layers=24, precision=abi.FP64, validate=True)
+    try:
+        b = _beyond_grid_batch()
+        ref = _bins_equal(rt, otables, b)
+        lv = slice(1, None)   # K = 2..LEV (K = 1 has no tpindex call)
+        assert ref["mt"][:, lv].min() >= 1 and ref["mt"][:, lv].max() <= 6
+        assert ref["mp"][:, lv].min() >= 1 and ref["mp"][:, lv].max() <= 50
+        assert ref["nh2o"][:, lv].min() >= 1 and ref["nh2o"][:, lv].max() <= 10
+        # the clamps are reached
+        assert set(ref["mt"][0, lv]) == {1} and set(ref["mt"][1, lv]) == {6}
+        assert set(ref["mp"][0, lv]) == {1} and set(ref["mp"][1, lv]) == {50}
+        assert set(ref["nh2o"][2, lv]) == {1} and set(ref["nh2o"][3, lv]) == {10}
+    finally:
+        rt.close()
+
+
+def test_planck_range_reported_without_validation(data_dir, otables):
+    """With validation off, a TLEV outside the Planck table still ends the
+    call with MGCM_RT_ETEMP: the kernels clamp the index INT(T*10-499) to
+    1..8501 and raise a status flag (code/sfluxi.f90:54-55).  The handle
+    stays usable, and the next batch matches the oracle."""
+    rt = abi.Radiation(data_dir, max_layers=24, precision=abi.FP64, validate=False)
+    try:
+        b = synth.make_batch(8, L=24, seed=44, cloud=True)
+        for t in (30.0, 950.0):
+            bad = dict(b)
+            bad["tlev"] = b["tlev"].copy()
+            bad["tlev"][5, 9] = t
+            with pytest.raises(abi.RTError) as e:
+                rt.run(bad)
+            assert e.value.code == -3
+        _check(b, rt.run(b), oracle.run_batch(otables, b))
+    finally:
+        rt.close()
