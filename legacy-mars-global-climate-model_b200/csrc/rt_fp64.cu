@@ -182,17 +182,6 @@ template __global__ void rt_fp64_screen<true>(SCREEN_ARGS);
 #undef SCREEN_ARGS
 
 // K2: solve the listed systems of one family, one thread per system.
-// Both solves ask for 7 resident CTAs per SM (72 registers), so the launch
-// grid -- 7 CTAs per SM, from the IR solve's occupancy -- is one wave of
-// either kernel.  Measured on the 64,800-column call: 11.68 -> 11.52 ms
-// MIXED, 12.00 -> 11.83 ms FP64, against 8 (64 registers) for the IR solve
-// and 6 (80) for the visible.
-#ifndef MGCM_IR_SOLVE_MINB
-#define MGCM_IR_SOLVE_MINB 7   // resident CTAs per SM asked of the IR solve
-#endif
-#ifndef MGCM_VIS_SOLVE_MINB
-#define MGCM_VIS_SOLVE_MINB 7  // the same for the visible solves (FP64 and MIXED)
-#endif
 template <bool VIS>
 __global__ void __launch_bounds__(128, VIS ? MGCM_VIS_SOLVE_MINB : MGCM_IR_SOLVE_MINB)
 rt_fp64_solve(const SegTable *__restrict__ st, int col_begin, int max_nl,

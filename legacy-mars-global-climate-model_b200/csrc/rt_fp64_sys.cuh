@@ -13,6 +13,19 @@ constexpr double PI_D = 3.1415926535897932;
 constexpr double TLIMITS = 1.0e-3;
 constexpr double TLIMITI = 5.0e-3;
 
+// Resident CTAs per SM (128 threads) asked of the solve kernels.  Both ask
+// for 7 (72 registers), so the grid the two solves of a part share -- 7 CTAs
+// per SM, from the IR solve's occupancy -- is one wave of either kernel.
+// Measured on the 64,800-column call: 11.68 -> 11.52 ms MIXED, 12.00 ->
+// 11.83 ms FP64, against 8 (64 registers) for the IR solve and 6 (80) for
+// the visible ones.
+#ifndef MGCM_IR_SOLVE_MINB
+#define MGCM_IR_SOLVE_MINB 7
+#endif
+#ifndef MGCM_VIS_SOLVE_MINB
+#define MGCM_VIS_SOLVE_MINB 7   // the FP64 and the MIXED visible solve
+#endif
+
 struct Lay {   // per-layer two-stream coefficients
     double gama, e1, e2, e3, e4, cp, cm, cpm1, cmm1;
 };

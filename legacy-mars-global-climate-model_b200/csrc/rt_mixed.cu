@@ -21,9 +21,6 @@
 
 namespace mgcm {
 
-#ifndef MGCM_VIS_SOLVE_MINB
-#define MGCM_VIS_SOLVE_MINB 7
-#endif
 __global__ void __launch_bounds__(128, MGCM_VIS_SOLVE_MINB)   // 72 registers, as the FP64 visible solve
 rt_mixed_solve_vis(const SegTable *__restrict__ st, int col_begin, int max_nl,
                unsigned char *__restrict__ blocks, size_t stride, const float *__restrict__ ktabf,
